@@ -1,0 +1,128 @@
+/*
+ * sdot_gpu.h -- C ABI of the B200-native power-diagram library (libsdot_b200.so).
+ *
+ * Drop-in for the power-diagram hot path of sdot (Laguerre cells of weighted
+ * Diracs clipped to a domain; cell integrals, centroids and the weight
+ * Hessian; Newton on the weights).  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Positions are AoS `double[n * dim]` (x0, y0[, z0], x1, ...), the layout
+ *    of the reference's Point2/Point3 arrays (src/sdot/Geometry/Point2.h:13-30).
+ *  - Indices are int64 (the reference's TI = std::size_t).
+ *  - `mem_space` says where a caller buffer lives: SDOT_HOST or SDOT_DEVICE
+ *    (a device pointer of the current CUDA device).
+ *  - Every call returns an sdot_status; sdot_last_error() gives the text.
+ *    No call aborts the process or traps the GPU.
+ *  - One context per stream; contexts are independent and may be used from
+ *    different threads.  A context is not re-entrant.
+ */
+#ifndef SDOT_GPU_H
+#define SDOT_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sdot_ctx sdot_ctx;
+
+typedef enum sdot_status {
+    SDOT_OK = 0,
+    SDOT_VOID_CELL = 1,       /* reference: for_each_laguerre_cell(stop_if_void) returns 1 */
+    SDOT_CAPACITY = 2,        /* a cell has more than 64 vertices (2D) */
+    SDOT_NOT_CONVERGED = 3,   /* Newton / PCG did not reach the tolerance */
+    SDOT_ITER_CAP = 4,        /* an iteration cap was reached */
+    SDOT_OOM = 5,
+    SDOT_BAD_ARG = 6,
+    SDOT_CUDA_ERROR = 7,
+    SDOT_UNSUPPORTED = 8
+} sdot_status;
+
+enum { SDOT_HOST = 0, SDOT_DEVICE = 1 };
+enum { SDOT_FP64 = 0, SDOT_MIXED = 1 };
+
+typedef struct sdot_options {
+    int64_t max_diracs_per_cell; /* SpZGrid( max_diracs_per_cell = 11 ), SpZGrid.h:37; 0 -> 11 */
+    void *stream;                /* cudaStream_t to run on; NULL -> the context creates its own */
+    int device;                  /* CUDA device ordinal; -1 -> current device */
+} sdot_options;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the pair (SpZGrid<Pc> grid, ConvexPolyhedronAssembly<Pc> bounds)
+ * that every reference entry point takes (SpZGrid.h:16-53,
+ * ConvexPolyhedronAssembly.h:12-51), with Pc::dim = dim and Pc::TF = double.
+ * precision: SDOT_FP64 (all arithmetic in double) or SDOT_MIXED (FP32
+ * clipping, FP64 re-clip and accumulation).                                  */
+sdot_ctx *sdot_create(int dim, int precision, const sdot_options *opt);
+void sdot_destroy(sdot_ctx *ctx);
+const char *sdot_last_error(const sdot_ctx *ctx);
+
+/* ---- Diracs --------------------------------------------------------------
+ * Replaces SpZGrid::update( positions, weights, nb_diracs, ... )
+ * (SpZGrid.tcc:24-38): the Z-order tree is rebuilt on the device.            */
+int sdot_set_diracs(sdot_ctx *ctx, const double *positions, const double *weights, int64_t n, int mem_space);
+/* New weights, same positions: only the per-node maximum weights change
+ * (SpZGrid::update with positions_have_changed = false).                     */
+int sdot_set_weights(sdot_ctx *ctx, const double *weights, int mem_space);
+
+/* ---- domain (cumulative, like PowerDiagram.add_..._shape) ---------------
+ * ConvexPolyhedronAssembly::add_box            (ConvexPolyhedronAssembly.tcc:46-50)
+ * ConvexPolyhedronAssembly::add_convex_polyhedron (:7-33): m (point, normal) half-planes
+ * ConvexPolyhedronAssembly::add_simplex        (:36-43): dim + 1 points
+ * ConvexPolyhedronAssembly::normalize          (:53-57)
+ * ConvexPolyhedronAssembly::measure            (:115-120) / ScaledImage::measure (ScaledImage.tcc:36-69)
+ * ScaledImage( min_pt, max_pt, data, sizes, nb_coeffs ) (ScaledImage.tcc:8-10): data is
+ *   x-fastest; nb_coeffs = 1 (piecewise constant).  Replaces the domain.   */
+int sdot_add_box_shape(sdot_ctx *ctx, const double *p0, const double *p1, double coeff);
+int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const double *normals, int64_t m,
+                                     double coeff);
+int sdot_add_simplex_shape(sdot_ctx *ctx, const double *points, double coeff);
+int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const double *data,
+                           const int64_t *sizes, int nb_coeffs);
+int sdot_clear_domain(sdot_ctx *ctx);
+int sdot_normalize_domain(sdot_ctx *ctx);
+int sdot_domain_measure(sdot_ctx *ctx, double *measure);
+
+/* ---- radial function ------------------------------------------------------
+ * on = 0: FunctionEnum::Unit (Unit.h:10-30); on = 1: FunctionEnum::InBallW05
+ * (InBallW05.h:8-28): each cell is also clipped by the disc of radius sqrt(w_i). */
+int sdot_set_ball_cut(sdot_ctx *ctx, int on);
+
+/* ---- per-cell results -----------------------------------------------------
+ * All three share one fused device evaluation (traversal + clipping +
+ * integrals + centroids + Hessian rows); it is recomputed only when the
+ * Diracs, weights, domain or radial function changed.
+ *
+ * get_integrals( res, grid, bounds, positions, weights, n, rf )   get_integrals.h:12-21
+ *   out: double[n] cell masses.                                               */
+int sdot_get_integrals(sdot_ctx *ctx, double *out, int mem_space);
+/* get_centroids( grid, bounds, positions, weights, n, rf, cb )     get_centroids.h:13-56
+ *   out_c: double[n * dim] centroids, out_m: double[n] masses (may be NULL). */
+int sdot_get_centroids(sdot_ctx *ctx, double *out_c, double *out_m, int mem_space);
+/* get_der_integrals_wrt_weights( offsets, columns, values, v_values, grid,
+ *   bounds, positions, weights, n, rf, stop_if_void )  get_der_integrals_wrt_weights.h:15-122
+ * Two-phase: call with columns == NULL to get *nnz_inout; then call with
+ * buffers of offsets[n + 1], columns[nnz], values[nnz], masses[n].
+ * Returns SDOT_VOID_CELL when stop_if_void and a cell is empty (the
+ * buffers are still filled).                                                  */
+int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t *columns, double *values,
+                                       double *masses, int64_t *nnz_inout, int stop_if_void, int mem_space);
+/* Cut ids of each final cell boundary, in vertex order (the CP2 cut_ids the
+ * traversal hands to its callback, SpZGrid.tcc:643): Dirac index, -1 for a
+ * domain edge, -2 for a disc arc.  Two-phase like the Hessian.               */
+int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *count_inout, int mem_space);
+
+/* Fused evaluation only, results kept on the device (for timing). */
+int sdot_evaluate(sdot_ctx *ctx);
+/* Device time in milliseconds of the last evaluation stages:
+ * t[0] tree build, t[1] cell kernel, t[2] Hessian assembly.                  */
+int sdot_last_timings(const sdot_ctx *ctx, double *t3);
+/* Number of cells rebuilt by the large-capacity fallback in the last evaluation. */
+int sdot_last_overflow_count(const sdot_ctx *ctx, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SDOT_GPU_H */

@@ -1,0 +1,754 @@
+// C ABI of libsdot_b200.so (include/sdot_gpu.h): context, domain, evaluation.
+#include "../../include/sdot_gpu.h"
+#include "cell2d.cuh"
+#include "csr.cuh"
+#include "geom2d.cuh"
+#include "prims.cuh"
+#include "tree.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace sdot;
+
+namespace {
+
+struct BadArg : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct Unsupported : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+template <class T>
+void dalloc(T *&p, size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    SDOT_CUDA(cudaMalloc(reinterpret_cast<void **>(&p), std::max<size_t>(count, 1) * sizeof(T) + 16));
+}
+template <class T>
+void dfree(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// A convex polygon of the domain: vertices (CCW) and the outward unit normal
+// of the edge leaving each vertex.
+struct Item2 {
+    std::vector<double> xy, nrm;
+    double coeff = 1;
+    double area() const {
+        // ConvexPolyhedron2::measure: fan from vertex 0 (ConvexPolyhedron2.tcc:1825-1832)
+        size_t n = xy.size() / 2;
+        double res = 0;
+        for (size_t i = 2; i < n; ++i) {
+            double ax = xy[0], ay = xy[1], bx = xy[2 * i - 2], by = xy[2 * i - 1], cx = xy[2 * i], cy = xy[2 * i + 1];
+            res += ax * (by - cy) + bx * (cy - ay) + cx * (ay - by);
+        }
+        return 0.5 * res;
+    }
+};
+
+// Host polygon used to build items with the same plane_cut as the kernels.
+struct HostPoly {
+    std::vector<double> x, y;
+    std::vector<int> id;
+    int n = 0;
+    explicit HostPoly(int cap) : x(cap), y(cap), id(cap) {}
+    PolyView<double> view() { return PolyView<double>{x.data(), y.data(), id.data(), 1}; }
+};
+
+const double kBoxNrm[4][2] = {{0, -1}, {1, 0}, {0, 1}, {-1, 0}};
+
+// ConvexPolyhedron2( Box ) (ConvexPolyhedron2.tcc:76-106)
+Item2 box_item(double x0, double y0, double x1, double y1, double coeff) {
+    Item2 it;
+    it.xy = {x0, y0, x1, y0, x1, y1, x0, y1};
+    for (auto &n : kBoxNrm) { it.nrm.push_back(n[0]); it.nrm.push_back(n[1]); }
+    it.coeff = coeff;
+    return it;
+}
+
+}  // namespace
+
+struct sdot_ctx {
+    int dim = 2, precision = SDOT_FP64, device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    long long max_per_leaf = 11;
+
+    long long n = 0, cap = 0;
+    double *d_pos = nullptr, *d_w = nullptr;
+    DeviceTree<2> tree2;
+    bool pos_dirty = true, w_dirty = true, dom_dirty = true, eval_dirty = true, nb_dirty = true;
+
+    // domain (host side)
+    std::vector<Item2> items;
+    bool has_image = false;
+    double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};
+    long long img_size[2] = {0, 0};
+    int img_ncoeffs = 1;
+    std::vector<double> img_data;
+    int ball = 0;
+
+    // domain (device side)
+    int mode = DM_SINGLE;
+    int start_n = 0;
+    double coeff = 1;
+    double *d_start = nullptr, *d_img = nullptr, *d_item_xy = nullptr, *d_item_nrm = nullptr, *d_item_coeff = nullptr;
+    int *d_item_off = nullptr;
+
+    // evaluation buffers
+    long long ecap = 0;
+    double *s_mass = nullptr, *s_mass_c = nullptr, *s_ctd = nullptr;
+    double *o_mass = nullptr, *o_mass_c = nullptr, *o_ctd = nullptr;
+    Rows rows, nb;             // Hessian rows, boundary id lists (sorted order)
+    long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
+    int *ovf_list = nullptr, *ovf_cnt = nullptr, *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;
+    unsigned *err = nullptr;
+    void *scratch = nullptr, *scan_tmp = nullptr;
+    long long nnz = 0, nb_total = 0;
+    long long n_void = 0;
+    int last_ovf = 0;
+    unsigned last_err = 0;
+    cudaEvent_t ev[4] = {};
+    float times[3] = {0, 0, 0};
+
+    ~sdot_ctx() {
+        cudaSetDevice(device);
+        tree2.release();
+        dfree(d_pos); dfree(d_w);
+        dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
+        free_eval();
+        for (auto &e : ev) if (e) cudaEventDestroy(e);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    void free_eval() {
+        dfree(s_mass); dfree(s_mass_c); dfree(s_ctd); dfree(o_mass); dfree(o_mass_c); dfree(o_ctd);
+        free_rows(rows);
+        free_rows(nb);
+        dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
+        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err);
+        if (scratch) cudaFree(scratch);
+        if (scan_tmp) cudaFree(scan_tmp);
+        scratch = scan_tmp = nullptr;
+        ecap = 0;
+    }
+
+    static void free_rows(Rows &r) {
+        dfree(r.cnt); dfree(r.col); dfree(r.val); dfree(r.side); dfree(r.side_col); dfree(r.side_val);
+        dfree(r.side_used);
+        r = Rows();
+    }
+    // ELL of `width` slots per row plus a side buffer for the few longer rows
+    static void alloc_rows(Rows &r, long long cap_n, int width, bool values) {
+        free_rows(r);
+        r.cap = width;
+        r.stride = cap_n;
+        r.side_cap = (1LL << 20) + cap_n / 8;
+        dalloc(r.cnt, cap_n);
+        dalloc(r.col, size_t(width) * cap_n);
+        dalloc(r.side, cap_n);
+        dalloc(r.side_col, r.side_cap);
+        if (values) {
+            dalloc(r.val, size_t(width) * cap_n);
+            dalloc(r.side_val, r.side_cap);
+        }
+        dalloc(r.side_used, 1);
+    }
+
+    void reserve_eval() {
+        if (ecap >= n && s_mass) return;
+        free_eval();
+        ecap = std::max<long long>(n, 1);
+        dalloc(s_mass, ecap); dalloc(s_mass_c, ecap); dalloc(s_ctd, 2 * ecap);
+        dalloc(o_mass, ecap); dalloc(o_mass_c, ecap); dalloc(o_ctd, 2 * ecap);
+        alloc_rows(rows, ecap, ROWCAP_2D, true);
+        dalloc(cnt_orig, ecap + 1);
+        dalloc(offsets, ecap + 1);
+        dalloc(ovf_list, ecap);
+        dalloc(ovf_cnt, 1);
+        dalloc(ovf_list2, ecap);
+        dalloc(ovf_cnt2, 1);
+        dalloc(err, 1);
+        SDOT_CUDA(cudaMalloc(&scratch, cells2d_scratch_bytes()));
+        SDOT_CUDA(cudaMalloc(&scan_tmp, scan_tmp_size(ecap + 1, sizeof(long long))));
+    }
+
+    void upload_domain() {
+        if (!dom_dirty) return;
+        if (has_image) {
+            mode = DM_IMAGE;
+            std::vector<double> st = {img_lo[0], img_lo[1], img_hi[0], img_lo[1], img_hi[0], img_hi[1], img_lo[0], img_hi[1]};
+            start_n = 4;
+            dalloc(d_start, 8);
+            SDOT_CUDA(cudaMemcpy(d_start, st.data(), 8 * sizeof(double), cudaMemcpyHostToDevice));
+            dalloc(d_img, img_data.size());
+            SDOT_CUDA(cudaMemcpy(d_img, img_data.data(), img_data.size() * sizeof(double), cudaMemcpyHostToDevice));
+            coeff = 1;
+        } else if (items.size() == 1) {
+            // ConvexPolyhedronAssembly::englobing_convex_polyhedron with one item
+            mode = DM_SINGLE;
+            const Item2 &it = items[0];
+            start_n = int(it.xy.size() / 2);
+            dalloc(d_start, it.xy.size());
+            SDOT_CUDA(cudaMemcpy(d_start, it.xy.data(), it.xy.size() * sizeof(double), cudaMemcpyHostToDevice));
+            coeff = it.coeff;
+        } else if (items.size() > 1) {
+            // englobing box inflated by its own size on each side (ConvexPolyhedronAssembly.tcc:60-92)
+            mode = DM_MULTI;
+            double mn[2] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max()};
+            double mx[2] = {-std::numeric_limits<double>::max(), -std::numeric_limits<double>::max()};
+            std::vector<int> off = {0};
+            std::vector<double> xy, nrm, co;
+            for (const Item2 &it : items) {
+                for (size_t k = 0; k < it.xy.size(); ++k) {
+                    mn[k % 2] = std::min(mn[k % 2], it.xy[k]);
+                    mx[k % 2] = std::max(mx[k % 2], it.xy[k]);
+                }
+                xy.insert(xy.end(), it.xy.begin(), it.xy.end());
+                nrm.insert(nrm.end(), it.nrm.begin(), it.nrm.end());
+                off.push_back(int(xy.size() / 2));
+                co.push_back(it.coeff);
+            }
+            double dx = mx[0] - mn[0], dy = mx[1] - mn[1];
+            Item2 eb = box_item(mn[0] - dx, mn[1] - dy, mx[0] + dx, mx[1] + dy, 1.0);
+            start_n = 4;
+            dalloc(d_start, 8);
+            SDOT_CUDA(cudaMemcpy(d_start, eb.xy.data(), 8 * sizeof(double), cudaMemcpyHostToDevice));
+            dalloc(d_item_off, off.size());
+            SDOT_CUDA(cudaMemcpy(d_item_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+            dalloc(d_item_xy, xy.size());
+            SDOT_CUDA(cudaMemcpy(d_item_xy, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice));
+            dalloc(d_item_nrm, nrm.size());
+            SDOT_CUDA(cudaMemcpy(d_item_nrm, nrm.data(), nrm.size() * sizeof(double), cudaMemcpyHostToDevice));
+            dalloc(d_item_coeff, co.size());
+            SDOT_CUDA(cudaMemcpy(d_item_coeff, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            throw BadArg("no domain: call sdot_add_box_shape (or another add_..._shape) first");
+        }
+        if (start_n > CAP_FAST_2D) throw Unsupported("domain polygon has more vertices than the cell capacity");
+        dom_dirty = false;
+    }
+
+    Cell2DArgs args() {
+        Cell2DArgs a;
+        a.n = n;
+        a.pos = tree2.pos;
+        a.w = tree2.w;
+        a.nodes = tree2.nodes;
+        a.start_n = start_n;
+        a.start_xy = d_start;
+        a.coeff = coeff;
+        a.mode = mode;
+        a.ball = ball;
+        a.img_lo[0] = img_lo[0]; a.img_lo[1] = img_lo[1];
+        a.img_hi[0] = img_hi[0]; a.img_hi[1] = img_hi[1];
+        a.img_nx = int(img_size[0]);
+        a.img_ny = int(img_size[1]);
+        a.img = d_img;
+        a.nitems = int(items.size());
+        a.item_off = d_item_off;
+        a.item_xy = d_item_xy;
+        a.item_nrm = d_item_nrm;
+        a.item_coeff = d_item_coeff;
+        a.ovf_list = ovf_list;
+        a.ovf_cnt = ovf_cnt;
+        a.ovf_list2 = ovf_list2;
+        a.ovf_cnt2 = ovf_cnt2;
+        a.err = err;
+        return a;
+    }
+
+    void ensure_tree() {
+        if (n == 0) throw BadArg("no Diracs: call sdot_set_diracs first");
+        if (pos_dirty) {
+            tree2.max_per_leaf = int(max_per_leaf);
+            tree2.build(d_pos, d_w, n, stream);
+            pos_dirty = w_dirty = false;
+        } else if (w_dirty) {
+            tree2.update_weights(d_w, stream);
+            w_dirty = false;
+        }
+    }
+
+    int evaluate() {
+        if (!eval_dirty) return finish_status();
+        if (dim != 2) throw Unsupported("dim 3 is not available in this build");
+        upload_domain();
+        reserve_eval();
+        if (!ev[0]) for (auto &e : ev) SDOT_CUDA(cudaEventCreate(&e));
+        SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
+        SDOT_CUDA(cudaEventRecord(ev[0], stream));
+        ensure_tree();
+        SDOT_CUDA(cudaEventRecord(ev[1], stream));
+        Cell2DArgs a = args();
+        a.mass = s_mass;
+        a.mass_c = s_mass_c;
+        a.ctd = s_ctd;
+        a.rows = rows;
+        cells2d_launch(a, scratch, stream);
+        SDOT_CUDA(cudaEventRecord(ev[2], stream));
+        csr_sort_merge(rows, n, tree2.idx, cnt_orig, stream);
+        scan_exclusive_total<long long>(cnt_orig, offsets, n, scan_tmp, stream);
+        unpermute(s_mass, o_mass, n, 1, tree2.idx, stream);
+        unpermute(s_mass_c, o_mass_c, n, 1, tree2.idx, stream);
+        unpermute(s_ctd, o_ctd, n, 2, tree2.idx, stream);
+        SDOT_CUDA(cudaEventRecord(ev[3], stream));
+        SDOT_CUDA(cudaMemcpyAsync(&nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaMemcpyAsync(&last_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaMemcpyAsync(&last_ovf, ovf_cnt, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaStreamSynchronize(stream));
+        SDOT_CUDA(cudaEventElapsedTime(&times[0], ev[0], ev[1]));
+        SDOT_CUDA(cudaEventElapsedTime(&times[1], ev[1], ev[2]));
+        SDOT_CUDA(cudaEventElapsedTime(&times[2], ev[2], ev[3]));
+        eval_dirty = false;
+        return finish_status();
+    }
+
+    int finish_status() {
+        if (last_err & DE_CAPACITY) {
+            last_error = "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
+            return SDOT_CAPACITY;
+        }
+        if (last_err & DE_STACK) {
+            last_error = "traversal stack overflow";
+            return SDOT_CAPACITY;
+        }
+        return SDOT_OK;
+    }
+
+    void evaluate_neighbors() {
+        if (!nb_dirty) return;
+        evaluate();
+        if (!nb.cnt || nb.stride < ecap) alloc_rows(nb, ecap, NBCAP_2D, false);
+        if (!nb_offsets) dalloc(nb_offsets, ecap + 1);
+        SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
+        Cell2DArgs a = args();
+        a.nb = nb;
+        cells2d_launch(a, scratch, stream);
+        nb_counts(nb, n, tree2.idx, cnt_orig, stream);
+        scan_exclusive_total<long long>(cnt_orig, nb_offsets, n, scan_tmp, stream);
+        SDOT_CUDA(cudaMemcpyAsync(&nb_total, nb_offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaStreamSynchronize(stream));
+        nb_dirty = false;
+    }
+
+    void copy_out(void *dst, const void *src, size_t bytes, int mem_space) {
+        SDOT_CUDA(cudaMemcpyAsync(dst, src, bytes, mem_space == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  stream));
+    }
+
+    void mark_dirty() { eval_dirty = nb_dirty = true; }
+};
+
+namespace {
+
+int fail(sdot_ctx *c, int code, const std::string &msg) {
+    if (c) c->last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(sdot_ctx *c, const F &f) {
+    if (!c) return SDOT_BAD_ARG;
+    try {
+        cudaSetDevice(c->device);
+        return f();
+    } catch (const CudaError &e) {
+        if (e.err == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return fail(c, SDOT_OOM, std::string("out of device memory in ") + e.where);
+        }
+        return fail(c, SDOT_CUDA_ERROR, std::string(cudaGetErrorString(e.err)) + " in " + e.where);
+    } catch (const BadArg &e) {
+        return fail(c, SDOT_BAD_ARG, e.what());
+    } catch (const Unsupported &e) {
+        return fail(c, SDOT_UNSUPPORTED, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(c, SDOT_OOM, "out of host memory");
+    } catch (const std::exception &e) {
+        return fail(c, SDOT_CUDA_ERROR, e.what());
+    }
+}
+
+void upload(double *dst, const double *src, size_t count, int mem_space, cudaStream_t st) {
+    SDOT_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(double),
+                              mem_space == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+}
+
+}  // namespace
+
+extern "C" {
+
+sdot_ctx *sdot_create(int dim, int precision, const sdot_options *opt) {
+    if (dim != 2 && dim != 3) return nullptr;
+    if (precision != SDOT_FP64 && precision != SDOT_MIXED) return nullptr;
+    sdot_ctx *c = nullptr;
+    try {
+        c = new sdot_ctx();
+    } catch (...) {
+        return nullptr;
+    }
+    c->dim = dim;
+    c->precision = precision;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (opt && opt->device >= 0) dev = opt->device;
+    c->device = dev;
+    if (opt && opt->max_diracs_per_cell > 0) c->max_per_leaf = opt->max_diracs_per_cell;
+    if (cudaSetDevice(dev) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    if (opt && opt->stream) {
+        c->stream = static_cast<cudaStream_t>(opt->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return nullptr;
+        }
+        c->own_stream = true;
+    }
+    return c;
+}
+
+void sdot_destroy(sdot_ctx *ctx) { delete ctx; }
+
+const char *sdot_last_error(const sdot_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int sdot_set_diracs(sdot_ctx *ctx, const double *positions, const double *weights, int64_t n, int mem_space) {
+    return guarded(ctx, [&] {
+        if (n < 0 || (n > 0 && (!positions || !weights))) throw BadArg("bad Dirac arrays");
+        if (n >= (1LL << 31) - 1) throw BadArg("at most 2^31 - 2 Diracs per context");
+        if (n > ctx->cap) {
+            dalloc(ctx->d_pos, size_t(ctx->dim) * n);
+            dalloc(ctx->d_w, size_t(n));
+            ctx->cap = n;
+        }
+        ctx->n = n;
+        if (n) {
+            upload(ctx->d_pos, positions, size_t(ctx->dim) * n, mem_space, ctx->stream);
+            upload(ctx->d_w, weights, size_t(n), mem_space, ctx->stream);
+        }
+        ctx->pos_dirty = ctx->w_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_set_weights(sdot_ctx *ctx, const double *weights, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!weights && ctx->n) throw BadArg("null weights");
+        if (ctx->n) upload(ctx->d_w, weights, size_t(ctx->n), mem_space, ctx->stream);
+        ctx->w_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_add_box_shape(sdot_ctx *ctx, const double *p0, const double *p1, double coeff) {
+    return guarded(ctx, [&] {
+        if (!p0 || !p1) throw BadArg("null box corner");
+        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        ctx->has_image = false;
+        ctx->items.push_back(box_item(p0[0], p0[1], p1[0], p1[1], coeff));
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const double *normals, int64_t m,
+                                     double coeff) {
+    return guarded(ctx, [&] {
+        if (m <= 0 || !points || !normals) throw BadArg("bad convex polyhedron");
+        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        // ConvexPolyhedronAssembly::add_convex_polyhedron: the bounding box of
+        // the points inflated by its size, cut by each (point, normal) half-plane.
+        double mn[2], mx[2];
+        for (int d = 0; d < 2; ++d) {
+            mn[d] = std::numeric_limits<double>::max();
+            mx[d] = -std::numeric_limits<double>::max();
+            for (int64_t i = 0; i < m; ++i) {
+                mn[d] = std::min(mn[d], points[2 * i + d]);
+                mx[d] = std::max(mx[d], points[2 * i + d]);
+            }
+        }
+        double dx = mx[0] - mn[0], dy = mx[1] - mn[1];
+        const int cap = int(4 + m + 2);
+        HostPoly hp(cap);
+        double bx[4] = {mn[0] - dx, mx[0] + dx, mx[0] + dx, mn[0] - dx};
+        double by[4] = {mn[1] - dy, mn[1] - dy, mx[1] + dy, mx[1] + dy};
+        for (int k = 0; k < 4; ++k) {
+            hp.x[k] = bx[k];
+            hp.y[k] = by[k];
+            hp.id[k] = -1 - k;
+        }
+        int nv = 4;
+        std::vector<double> un(2 * m);
+        for (int64_t i = 0; i < m; ++i) {
+            // Point2 normalized(): p / (|p| + 1e-40)
+            double nx = normals[2 * i], ny = normals[2 * i + 1];
+            double d = std::sqrt(nx * nx + ny * ny) + 1e-40;
+            un[2 * i] = nx / d;
+            un[2 * i + 1] = ny / d;
+            nv = plane_cut(hp.view(), nv, cap, points[2 * i], points[2 * i + 1], un[2 * i], un[2 * i + 1], int(i), false);
+            if (nv <= 0) break;
+        }
+        if (nv <= 0) throw BadArg("empty convex polyhedron");
+        Item2 it;
+        it.coeff = coeff;
+        for (int k = 0; k < nv; ++k) {
+            it.xy.push_back(hp.x[k]);
+            it.xy.push_back(hp.y[k]);
+            int id = hp.id[k];
+            if (id >= 0) {
+                it.nrm.push_back(un[2 * id]);
+                it.nrm.push_back(un[2 * id + 1]);
+            } else {
+                it.nrm.push_back(kBoxNrm[-1 - id][0]);
+                it.nrm.push_back(kBoxNrm[-1 - id][1]);
+            }
+        }
+        ctx->has_image = false;
+        ctx->items.push_back(std::move(it));
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_add_simplex_shape(sdot_ctx *ctx, const double *pts, double coeff) {
+    return guarded(ctx, [&] {
+        if (!pts) throw BadArg("null simplex");
+        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        // ConvexPolyhedron2( Simplex ) (ConvexPolyhedron2.tcc:19-60)
+        double p[3][2] = {{pts[0], pts[1]}, {pts[2], pts[3]}, {pts[4], pts[5]}};
+        double cx = 1.0 / 3 * (p[0][0] + p[1][0] + p[2][0]), cy = 1.0 / 3 * (p[0][1] + p[1][1] + p[2][1]);
+        auto nrm = [](const double *a, const double *b, double *o) {
+            double vx = a[0] - b[0], vy = a[1] - b[1];
+            double rx = -vy, ry = vx;  // rot90
+            double l = std::sqrt(rx * rx + ry * ry);
+            o[0] = rx / l;
+            o[1] = ry / l;
+        };
+        double n0[2], n1[2], n2[2];
+        nrm(p[0], p[1], n0);
+        nrm(p[1], p[2], n1);
+        nrm(p[2], p[0], n2);
+        Item2 it;
+        it.coeff = coeff;
+        if ((p[0][0] - cx) * n0[0] + (p[0][1] - cy) * n0[1] < 0) {
+            it.xy = {p[0][0], p[0][1], p[2][0], p[2][1], p[1][0], p[1][1]};
+            it.nrm = {-n2[0], -n2[1], -n1[0], -n1[1], -n0[0], -n0[1]};
+        } else {
+            it.xy = {p[0][0], p[0][1], p[1][0], p[1][1], p[2][0], p[2][1]};
+            it.nrm = {n0[0], n0[1], n1[0], n1[1], n2[0], n2[1]};
+        }
+        ctx->has_image = false;
+        ctx->items.push_back(std::move(it));
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const double *data,
+                           const int64_t *sizes, int nb_coeffs) {
+    return guarded(ctx, [&] {
+        if (!min_pt || !max_pt || !data || !sizes) throw BadArg("null image argument");
+        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        if (nb_coeffs != 1) throw Unsupported("only piecewise-constant images (nb_coeffs = 1) are available");
+        if (sizes[0] <= 0 || sizes[1] <= 0) throw BadArg("bad image size");
+        ctx->items.clear();
+        ctx->has_image = true;
+        for (int d = 0; d < 2; ++d) {
+            ctx->img_lo[d] = min_pt[d];
+            ctx->img_hi[d] = max_pt[d];
+            ctx->img_size[d] = sizes[d];
+        }
+        ctx->img_ncoeffs = nb_coeffs;
+        ctx->img_data.assign(data, data + sizes[0] * sizes[1] * nb_coeffs);
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_clear_domain(sdot_ctx *ctx) {
+    return guarded(ctx, [&] {
+        ctx->items.clear();
+        ctx->has_image = false;
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+static double domain_measure(const sdot_ctx *ctx) {
+    if (ctx->has_image) {
+        // ScaledImage::measure (ScaledImage.tcc:36-69), nb_coeffs == 1: mean * volume
+        double s = 0;
+        for (double v : ctx->img_data) s += v;
+        s /= double(ctx->img_data.size());
+        for (int d = 0; d < 2; ++d) s *= ctx->img_hi[d] - ctx->img_lo[d];
+        return s;
+    }
+    double res = 0;
+    for (const Item2 &it : ctx->items) res += it.coeff * it.area();
+    return res;
+}
+
+int sdot_normalize_domain(sdot_ctx *ctx) {
+    return guarded(ctx, [&] {
+        double mea = domain_measure(ctx);
+        if (mea != 0) {
+            if (ctx->has_image)
+                for (double &v : ctx->img_data) v /= mea;
+            else
+                for (Item2 &it : ctx->items) it.coeff /= mea;
+        }
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_domain_measure(sdot_ctx *ctx, double *measure) {
+    return guarded(ctx, [&] {
+        if (!measure) throw BadArg("null output");
+        *measure = domain_measure(ctx);
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_set_ball_cut(sdot_ctx *ctx, int on) {
+    return guarded(ctx, [&] {
+        ctx->ball = on ? 1 : 0;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_evaluate(sdot_ctx *ctx) {
+    return guarded(ctx, [&] { return ctx->evaluate(); });
+}
+
+int sdot_get_integrals(sdot_ctx *ctx, double *out, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!out) throw BadArg("null output");
+        int st = ctx->evaluate();
+        ctx->copy_out(out, ctx->o_mass, size_t(ctx->n) * sizeof(double), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return st;
+    });
+}
+
+int sdot_get_centroids(sdot_ctx *ctx, double *out_c, double *out_m, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!out_c) throw BadArg("null output");
+        int st = ctx->evaluate();
+        ctx->copy_out(out_c, ctx->o_ctd, size_t(ctx->n) * ctx->dim * sizeof(double), mem_space);
+        if (out_m) ctx->copy_out(out_m, ctx->o_mass_c, size_t(ctx->n) * sizeof(double), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return st;
+    });
+}
+
+int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t *columns, double *values,
+                                       double *masses, int64_t *nnz_inout, int stop_if_void, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!nnz_inout) throw BadArg("null nnz");
+        int st = ctx->evaluate();
+        if (st != SDOT_OK) return st;
+        if (!columns) {
+            *nnz_inout = ctx->nnz;
+            return int(SDOT_OK);
+        }
+        if (*nnz_inout < ctx->nnz) throw BadArg("columns/values buffers smaller than nnz");
+        if (!offsets || !values || !masses) throw BadArg("null output");
+        const long long n = ctx->n, nnz = ctx->nnz;
+        long long *dcols = reinterpret_cast<long long *>(columns);
+        double *dvals = values;
+        long long *tmp_c = nullptr;
+        double *tmp_v = nullptr;
+        if (mem_space != SDOT_DEVICE) {
+            dalloc(tmp_c, nnz);
+            dalloc(tmp_v, nnz);
+            dcols = tmp_c;
+            dvals = tmp_v;
+        }
+        csr_write(ctx->rows, n, ctx->tree2.idx, ctx->offsets, dcols, dvals, ctx->stream);
+        if (mem_space != SDOT_DEVICE) {
+            SDOT_CUDA(cudaMemcpyAsync(columns, tmp_c, nnz * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(values, tmp_v, nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        ctx->copy_out(offsets, ctx->offsets, size_t(n + 1) * sizeof(long long), mem_space);
+        ctx->copy_out(masses, ctx->o_mass, size_t(n) * sizeof(double), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        dfree(tmp_c);
+        dfree(tmp_v);
+        *nnz_inout = nnz;
+        if (stop_if_void) {
+            // reference: any v == 0 -> 1 (get_der_integrals_wrt_weights.h:93-96)
+            std::vector<double> m(n);
+            SDOT_CUDA(cudaMemcpy(m.data(), ctx->o_mass, n * sizeof(double), cudaMemcpyDeviceToHost));
+            for (double v : m)
+                if (v == 0) {
+                    ctx->last_error = "void cell";
+                    return int(SDOT_VOID_CELL);
+                }
+        }
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *count_inout, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!count_inout) throw BadArg("null count");
+        ctx->evaluate_neighbors();
+        if (!ids) {
+            *count_inout = ctx->nb_total;
+            return int(SDOT_OK);
+        }
+        if (*count_inout < ctx->nb_total) throw BadArg("ids buffer smaller than count");
+        if (!offsets) throw BadArg("null offsets");
+        const long long n = ctx->n, tot = ctx->nb_total;
+        long long *dids = reinterpret_cast<long long *>(ids);
+        long long *tmp = nullptr;
+        if (mem_space != SDOT_DEVICE) {
+            dalloc(tmp, tot);
+            dids = tmp;
+        }
+        nb_write(ctx->nb, n, ctx->tree2.idx, ctx->nb_offsets, dids, ctx->stream);
+        if (mem_space != SDOT_DEVICE)
+            SDOT_CUDA(cudaMemcpyAsync(ids, tmp, tot * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+        ctx->copy_out(offsets, ctx->nb_offsets, size_t(n + 1) * sizeof(long long), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        dfree(tmp);
+        *count_inout = tot;
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_last_timings(const sdot_ctx *ctx, double *t3) {
+    if (!ctx || !t3) return SDOT_BAD_ARG;
+    for (int k = 0; k < 3; ++k) t3[k] = ctx->times[k];
+    return SDOT_OK;
+}
+
+int sdot_last_overflow_count(const sdot_ctx *ctx, int64_t *count) {
+    if (!ctx || !count) return SDOT_BAD_ARG;
+    *count = ctx->last_ovf;
+    return SDOT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,559 @@
+// 2D Laguerre-cell kernels (sm_100a), FP64.
+//
+// One thread builds one cell.  Threads take Diracs in Morton (sorted) order so
+// a warp works on 32 neighbouring cells and walks nearly the same tree nodes.
+// The fast tier keeps the cell polygon in shared memory (SoA, one column per
+// thread); cells that outgrow it are rebuilt by the big and huge tiers whose
+// polygons live in global scratch (one column per thread, coalesced).  The
+// traversal stack lives in local memory.
+//
+// Reference behaviour restated here:
+//  * traversal, eviction test and bisector cuts: SpZGrid::for_each_laguerre_cell
+//    (src/sdot/PowerDiagram/Visitors/SpZGrid.tcc:494-719, eviction :475-480,
+//    bisector :506-522); the reference pops boxes best-first from a priority
+//    queue keyed on the float distance to the box centre, here a depth-first
+//    walk pushes children farthest-first so the nearest is visited first.
+//  * disc clipping (InBallW05, ball_cut after all plane cuts): :633-634.
+//  * integrals: ConvexPolyhedron2::integration(Constant,Unit)
+//    (ConvexPolyhedron2.tcc:1791-1843), add_centroid_contrib (:1047-1074),
+//    for_each_boundary_item (:437-478).
+//  * Hessian row: get_der_integrals_wrt_weights (get_der_integrals_wrt_weights.h:43-88):
+//    off-diagonal -1/2 * len_ij / |x_i - x_j|, diagonal the sum of those plus
+//    1/2 * arc_len / sqrt(w_i).
+//  * bounds: ConvexPolyhedronAssembly::for_each_intersection
+//    (ConvexPolyhedronAssembly.tcc:132-142) and ScaledImage::for_each_intersection
+//    (ScaledImage.tcc:98-149).  A piece (cell intersected with an item or a
+//    pixel) is produced by clipping the cell by the item/pixel half-planes,
+//    which is the same convex set the reference gets by clipping the item by
+//    the cell's lines.
+#include "cell2d.cuh"
+#include "geom2d.cuh"
+
+namespace sdot {
+
+namespace {
+
+constexpr int T2D = 64;     // threads per block of the fast kernel
+constexpr int STACK = 64;   // traversal stack (depth <= 17 levels, <= 3 pending siblings each)
+constexpr int BIG_THREADS = 148 * 64;
+constexpr int HUGE_THREADS = 148 * 4;
+
+// Destination of one row (or id list): element k at col[k * stride]
+// (col == nullptr: the output is not wanted, only counted).
+struct Out {
+    int *col;
+    double *val;
+    long long stride;
+    int cap;
+    int cnt = 0;
+    SDOT_HDI Out(int *c, double *v, long long st, int cp) : col(c), val(v), stride(st), cap(cp) {}
+    SDOT_HDI void emit(int j, double v) {
+        if (col && cnt < cap) {
+            col[cnt * stride] = j;
+            if (val) val[cnt * stride] = v;
+        }
+        ++cnt;
+    }
+    SDOT_HDI bool ok() const { return !col || cnt <= cap; }
+};
+
+// Integrates a streamed polygon (one piece at a time) and collects the
+// boundary measures for the Hessian row.
+template <bool DIRECT>
+struct Sink {
+    const PolyView<double> &cell;
+    const double *pos;
+    double c0x, c0y, sqw0;
+    double cx, cy, r;
+    double coeff = 1.0;
+    // piece state
+    bool has_first = false;
+    double fx = 0, fy = 0, px = 0, py = 0;
+    int ft = 0, pt = 0, cnt = 0;
+    double tr2 = 0, arcs = 0, pm = 0, pcx = 0, pcy = 0;
+    // cell totals
+    double mass = 0, mass_c = 0, momx = 0, momy = 0, der0 = 0;
+    // rows: DIRECT emits one item per line edge; otherwise measures are
+    // summed per cell edge in acc (negative = edge not seen yet)
+    double *acc;
+    int acc_st;
+    Out &row;
+
+    SDOT_HDI Sink(const PolyView<double> &c, const double *p, double x0, double y0, double sw, double r_, double *a,
+                    int ast, Out &ro)
+        : cell(c), pos(p), c0x(x0), c0y(y0), sqw0(sw), cx(x0), cy(y0), r(r_), acc(a), acc_st(ast), row(ro) {}
+
+    SDOT_HDI void begin_piece(double c) {
+        coeff = c;
+        has_first = false;
+        cnt = 0;
+        tr2 = arcs = pm = pcx = pcy = 0;
+    }
+    SDOT_HDI void line(int t, double len) {
+        if (t < 0) return;
+        const int id = cell.I(t);
+        if (id < 0) return;
+        const double m = coeff * len;
+        if (DIRECT) {
+            const double dx = c0x - pos[2 * id], dy = c0y - pos[2 * id + 1];
+            const double dist = sqrt(dx * dx + dy * dy);
+            if (dist != 0) {
+                const double b = 0.5 * m / dist;
+                row.emit(id, -b);
+                der0 += b;
+            }
+        } else {
+            double &a = acc[t * acc_st];
+            a = a < 0 ? m : a + m;
+        }
+    }
+    SDOT_HDI void edge(double ax, double ay, int t, double bx, double by) {
+        if (t == ID_ARC) {
+            arcs += arc_area(ax, ay, bx, by, cx, cy, r);
+            centroid_arc(pcx, pcy, pm, ax, ay, bx, by, cx, cy, r, coeff);
+            double a0;
+            const double a1 = arc_angles(ax, ay, bx, by, cx, cy, a0);
+            der0 += 0.5 * (coeff * (a1 - a0) * r) / sqw0;
+        } else {
+            const double dx = bx - ax, dy = by - ay;
+            line(t, sqrt(dx * dx + dy * dy));
+        }
+    }
+    SDOT_HDI void push(double x, double y, int tag) {
+        if (!has_first) {
+            has_first = true;
+            fx = x; fy = y; ft = tag;
+        } else {
+            edge(px, py, pt, x, y);
+        }
+        if (++cnt >= 3) {
+            const double t2 = fx * (py - y) + px * (y - fy) + x * (fy - py);
+            tr2 += t2;
+            const double lea = 0.5 * t2 * coeff;
+            const double f = (1.0 / 3.0) * lea;
+            pcx += f * (fx + px + x);
+            pcy += f * (fy + py + y);
+            pm += lea;
+        }
+        px = x; py = y; pt = tag;
+    }
+    SDOT_HDI void finish() {
+        if (has_first) edge(px, py, pt, fx, fy);
+    }
+    // radius: the disc radius after clipping (> 0 keeps a vertex-free piece
+    // as the full disc), or -1 when there is no disc.
+    SDOT_HDI void end_piece(double radius) {
+        if (cnt == 0) {
+            if (radius > 0) {
+                const double lea = kPi * (radius * radius) * coeff;
+                mass += lea;
+                mass_c += lea;
+                momx += lea * cx;
+                momy += lea * cy;
+                der0 += 0.5 * (coeff * 2 * kPi * radius) / sqw0;
+            }
+            return;
+        }
+        mass += coeff * (tr2 * 0.5 + arcs);
+        mass_c += pm;
+        momx += pcx;
+        momy += pcy;
+    }
+};
+
+// Records the ids of the streamed (disc-clipped) cell boundary.
+struct NbSink {
+    const PolyView<double> &cell;
+    Out &out;
+    SDOT_HDI NbSink(const PolyView<double> &c, Out &o) : cell(c), out(o) {}
+    SDOT_HDI void push(double, double, int tag) { out.emit(tag == ID_ARC ? ID_ARC : cell.I(tag), 0.0); }
+    SDOT_HDI void finish() {}
+};
+
+// Streams a polygon; each vertex carries the index of the cell edge leaving
+// it: for the cell itself that is the vertex index, for a piece (a clipped
+// copy of the cell) it is the tag stored in its id slot.
+template <class Stage>
+SDOT_HDI void stream_cell(const PolyView<double> &cell, int n, Stage &st) {
+    for (int k = 0; k < n; ++k) st.push(cell.X(k), cell.Y(k), k);
+    st.finish();
+}
+template <class Stage>
+SDOT_HDI void stream_piece(const PolyView<double> &piece, int n, Stage &st) {
+    for (int k = 0; k < n; ++k) st.push(piece.X(k), piece.Y(k), piece.I(k));
+    st.finish();
+}
+
+// Builds the Laguerre cell of sorted Dirac s (before any disc clipping).
+// Returns the vertex count, or -1 on capacity overflow.
+SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double c0x, double c0y,
+                          double w0) {
+    int n = A.start_n;
+    for (int k = 0; k < n; ++k) {
+        cell.X(k) = A.start_xy[2 * k];
+        cell.Y(k) = A.start_xy[2 * k + 1];
+        cell.I(k) = domain_id(k);
+    }
+    int stack[STACK];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int node = stack[--sp];
+        const TreeNode<2> nd = A.nodes[node];
+        // SpZGrid::can_be_evicted: skip the box when no Dirac in it can be
+        // closer (in power distance) than c0 to any current vertex.
+        bool evict = true;
+        for (int k = 0; k < n; ++k) {
+            const double px = cell.X(k), py = cell.Y(k);
+            const double qx = fmin(nd.hi[0], fmax(nd.lo[0], px));
+            const double qy = fmin(nd.hi[1], fmax(nd.lo[1], py));
+            const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
+            const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - nd.maxw;
+            if (!(lhs <= rhs)) {
+                evict = false;
+                break;
+            }
+        }
+        if (evict) continue;
+        if (nd.b < 0) {
+            const int first = nd.a, nch = -nd.b;
+            float key[4];
+            int ch[4];
+            for (int c = 0; c < nch; ++c) {
+                const TreeNode<2> &cn = A.nodes[first + c];
+                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
+                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
+                key[c] = float(mx * mx + my * my);
+                ch[c] = first + c;
+            }
+            // insertion sort, farthest first
+            for (int i = 1; i < nch; ++i) {
+                const float kk = key[i];
+                const int cc = ch[i];
+                int j = i - 1;
+                while (j >= 0 && key[j] < kk) {
+                    key[j + 1] = key[j];
+                    ch[j + 1] = ch[j];
+                    --j;
+                }
+                key[j + 1] = kk;
+                ch[j + 1] = cc;
+            }
+            if (sp + nch > STACK) {
+                flag_error(A.err, DE_STACK);
+                return -1;
+            }
+            for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
+        } else {
+            for (int j = nd.a; j < nd.b; ++j) {
+                if (j == s) continue;
+                const double c1x = A.pos[2 * j], c1y = A.pos[2 * j + 1], w1 = A.w[j];
+                double ox, oy, nx, ny;
+                bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
+                n = plane_cut(cell, n, cap, ox, oy, nx, ny, j, true);
+                if (n <= 0) return n;
+            }
+        }
+    }
+    return n;
+}
+
+// Full per-cell work.  Returns false when a capacity was exceeded (the cell
+// is then rebuilt by the next tier, which rewrites every output of it).
+template <int MODE, bool BALL>
+SDOT_KFN bool process_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double *acc,
+                             int acc_st, const PolyView<double> &piece, Out &row, Out &nbo) {
+    const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
+    const int n = build_cell(A, s, cell, cap, c0x, c0y, w0);
+    if (n < 0) return false;
+
+    const double r = BALL ? sqrt(w0) : -1.0;
+    constexpr bool DIRECT = MODE == DM_SINGLE;
+    Sink<DIRECT> sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
+
+    if (MODE == DM_SINGLE && !BALL) {
+        // reference order: fan from vertex 0, boundary items from edge (n-1 -> 0)
+        double tr2 = 0;
+        for (int i = 2; i < n; ++i) {
+            const double ax = cell.X(0), ay = cell.Y(0);
+            const double bx = cell.X(i - 1), by = cell.Y(i - 1), cx = cell.X(i), cy = cell.Y(i);
+            const double t2 = ax * (by - cy) + bx * (cy - ay) + cx * (ay - by);
+            tr2 += t2;
+            const double lea = 0.5 * t2 * A.coeff;
+            const double f = (1.0 / 3.0) * lea;
+            sink.momx += f * (ax + bx + cx);
+            sink.momy += f * (ay + by + cy);
+            sink.mass_c += lea;
+        }
+        sink.mass = A.coeff * (tr2 * 0.5);
+        sink.begin_piece(A.coeff);
+        for (int i1 = 0, i0 = n - 1; i1 < n; i0 = i1++) {
+            const double dx = cell.X(i1) - cell.X(i0), dy = cell.Y(i1) - cell.Y(i0);
+            sink.line(i0, sqrt(dx * dx + dy * dy));
+        }
+    } else if (MODE == DM_SINGLE) {
+        sink.begin_piece(A.coeff);
+        DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
+        stream_cell(cell, n, dc);
+        sink.end_piece(dc.result_radius());
+    } else {
+        for (int k = 0; k < n; ++k) acc[k * acc_st] = -1.0;
+        if (n > 0) {
+            if (MODE == DM_IMAGE) {
+                double xmin = cell.X(0), xmax = xmin, ymin = cell.Y(0), ymax = ymin;
+                for (int k = 1; k < n; ++k) {
+                    xmin = fmin(xmin, cell.X(k)); xmax = fmax(xmax, cell.X(k));
+                    ymin = fmin(ymin, cell.Y(k)); ymax = fmax(ymax, cell.Y(k));
+                }
+                if (BALL) {
+                    xmin = fmax(xmin, c0x - r); xmax = fmin(xmax, c0x + r);
+                    ymin = fmax(ymin, c0y - r); ymax = fmin(ymax, c0y + r);
+                }
+                const double psx = (A.img_hi[0] - A.img_lo[0]) / A.img_nx;
+                const double psy = (A.img_hi[1] - A.img_lo[1]) / A.img_ny;
+                // pixels outside the cell's bounding box give empty pieces
+                int ix0 = int(floor((xmin - A.img_lo[0]) / psx)), ix1 = int(floor((xmax - A.img_lo[0]) / psx));
+                int iy0 = int(floor((ymin - A.img_lo[1]) / psy)), iy1 = int(floor((ymax - A.img_lo[1]) / psy));
+                ix0 = max(ix0, 0); iy0 = max(iy0, 0);
+                ix1 = min(ix1, A.img_nx - 1); iy1 = min(iy1, A.img_ny - 1);
+                for (int iy = iy0; iy <= iy1; ++iy) {
+                    const double y0 = A.img_lo[1] + psy * double(iy), y1 = A.img_lo[1] + psy * double(iy + 1);
+                    for (int ix = ix0; ix <= ix1; ++ix) {
+                        const double x0 = A.img_lo[0] + psx * double(ix), x1 = A.img_lo[0] + psx * double(ix + 1);
+                        sink.begin_piece(A.img[(long long)iy * A.img_nx + ix]);
+                        if (BALL) {
+                            DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
+                            AxisClip<DiscClip<Sink<DIRECT>>> c4(dc, 1, y1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>> c3(c4, 1, y0, 1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                            stream_cell(cell, n, c1);
+                            sink.end_piece(dc.result_radius());
+                        } else {
+                            AxisClip<Sink<DIRECT>> c4(sink, 1, y1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<Sink<DIRECT>>> c3(c4, 1, y0, 1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<Sink<DIRECT>>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<AxisClip<Sink<DIRECT>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                            stream_cell(cell, n, c1);
+                            sink.end_piece(-1.0);
+                        }
+                    }
+                }
+            } else {  // DM_MULTI
+                for (int it = 0; it < A.nitems; ++it) {
+                    int np = n;
+                    for (int k = 0; k < n; ++k) {
+                        piece.X(k) = cell.X(k);
+                        piece.Y(k) = cell.Y(k);
+                        piece.I(k) = k;
+                    }
+                    for (int e = A.item_off[it]; e < A.item_off[it + 1] && np > 0; ++e)
+                        np = plane_cut(piece, np, cap, A.item_xy[2 * e], A.item_xy[2 * e + 1], A.item_nrm[2 * e],
+                                       A.item_nrm[2 * e + 1], PID_OWN, false);
+                    if (np < 0) return false;
+                    sink.begin_piece(A.item_coeff[it]);
+                    if (BALL) {
+                        DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
+                        stream_piece(piece, np, dc);
+                        sink.end_piece(dc.result_radius());
+                    } else {
+                        stream_piece(piece, np, sink);
+                        sink.end_piece(-1.0);
+                    }
+                }
+            }
+        }
+        if (A.rows.cnt) {
+            for (int i1 = 0, i0 = n - 1; i1 < n; i0 = i1++) {
+                const double m = acc[i0 * acc_st];
+                if (m < 0) continue;
+                const int id = cell.I(i0);
+                const double dx = c0x - A.pos[2 * id], dy = c0y - A.pos[2 * id + 1];
+                const double dist = sqrt(dx * dx + dy * dy);
+                if (dist != 0) {
+                    const double b = 0.5 * m / dist;
+                    row.emit(id, -b);
+                    sink.der0 += b;
+                }
+            }
+        }
+    }
+
+    if (A.rows.cnt) {
+        row.emit(int(s), sink.der0);
+        if (!row.ok()) return false;
+    }
+    if (A.nb.cnt) {
+        if (BALL) {
+            NbSink nbs(cell, nbo);
+            DiscClip<NbSink> dc(nbs, c0x, c0y, r);
+            stream_cell(cell, n, dc);
+        } else {
+            for (int k = 0; k < n; ++k) nbo.emit(cell.I(k), 0.0);
+        }
+        if (!nbo.ok()) return false;
+    }
+    if (A.mass) A.mass[s] = sink.mass;
+    if (A.mass_c) A.mass_c[s] = sink.mass_c;
+    if (A.ctd) {
+        const double d = sink.mass_c + (sink.mass_c == 0);
+        A.ctd[2 * s] = sink.momx / d;
+        A.ctd[2 * s + 1] = sink.momy / d;
+    }
+    return true;
+}
+
+// shared memory of the fast kernel, in half-doubles per vertex slot and
+// thread beyond x, y, id: acc (image, multi) and the piece polygon (multi)
+template <int MODE>
+constexpr int smem_extra_halves() {
+    return MODE == DM_SINGLE ? 0 : (MODE == DM_IMAGE ? 2 : 8);
+}
+
+template <int MODE, bool BALL>
+__global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
+    extern __shared__ double smem[];
+    constexpr int CAP = CAP_FAST_2D;
+    const int t = threadIdx.x;
+    double *sx = smem;
+    double *sy = sx + CAP * T2D;
+    int *sid = reinterpret_cast<int *>(sy + CAP * T2D);
+    double *extra = sy + CAP * T2D + (CAP * T2D + 1) / 2;
+    PolyView<double> cell{sx + t, sy + t, sid + t, T2D};
+    double *acc = extra + t;
+    PolyView<double> piece{extra + CAP * T2D + t, extra + 2 * CAP * T2D + t,
+                           reinterpret_cast<int *>(extra + 3 * CAP * T2D) + t, T2D};
+    const long long s = blockIdx.x * (long long)T2D + t;
+    if (s >= A.n) return;
+    Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
+    Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
+    if (process_cell<MODE, BALL>(A, s, cell, CAP, acc, T2D, piece, row, nbo)) {
+        if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
+        if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
+    } else {
+        const int k = atomicAdd(A.ovf_cnt, 1);
+        A.ovf_list[k] = int(s);
+    }
+}
+
+// Scratch layout of one large tier: `S` threads, polygon capacity `cap`.
+struct TierScratch {
+    PolyView<double> cell, piece;
+    double *acc;
+    int *row_col;
+    double *row_val;
+    int *nb_id;
+    SDOT_HDI TierScratch(double *base, long long S, int cap, int g) {
+        double *p = base;
+        cell = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S)};
+        p += 3 * cap * S;
+        acc = p + g;
+        p += cap * S;
+        piece = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S)};
+        p += 3 * cap * S;
+        row_val = p + g;
+        p += (cap + 1) * S;
+        row_col = reinterpret_cast<int *>(p) + g;
+        p += (cap + 1) * S;
+        nb_id = reinterpret_cast<int *>(p) + g;
+    }
+};
+// doubles of one tier's scratch: cell (3 cap), acc (cap), piece (3 cap),
+// row values (cap + 1), row columns (cap + 1, ints in double slots), ids (2 cap ints)
+__host__ __device__ constexpr long long tier_doubles(long long S, int cap) {
+    return S * (7LL * cap + 2LL * (cap + 1) + 2LL * cap);
+}
+
+// Copies a finished row from tier scratch to its ELL slot or the side buffer.
+__device__ bool commit(const Rows &R, long long s, const int *col, const double *val, long long st, int cnt) {
+    if (cnt <= R.cap) {
+        for (int k = 0; k < cnt; ++k) {
+            R.col[k * R.stride + s] = col[k * st];
+            if (R.val) R.val[k * R.stride + s] = val[k * st];
+        }
+    } else {
+        const unsigned long long off = atomicAdd(R.side_used, (unsigned long long)cnt);
+        if ((long long)(off + cnt) > R.side_cap) return false;
+        R.side[s] = (long long)off;
+        for (int k = 0; k < cnt; ++k) {
+            R.side_col[off + k] = col[k * st];
+            if (R.side_val) R.side_val[off + k] = val[k * st];
+        }
+    }
+    R.cnt[s] = cnt;
+    return true;
+}
+
+template <int MODE, bool BALL, int CAP>
+__global__ void __launch_bounds__(64) k_cells2d_tier(const Cell2DArgs A, double *scratch, int nthreads, const int *list,
+                                                     const int *list_cnt, int *next_list, int *next_cnt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nthreads) return;
+    TierScratch T(scratch, nthreads, CAP, g);
+    const int cnt = *list_cnt;
+    for (int i = g; i < cnt; i += nthreads) {
+        const long long s = list[i];
+        Out row(A.rows.cnt ? T.row_col : nullptr, T.row_val, nthreads, CAP + 1);
+        Out nbo(A.nb.cnt ? T.nb_id : nullptr, nullptr, nthreads, 2 * CAP);
+        bool ok = process_cell<MODE, BALL>(A, s, T.cell, CAP, T.acc, nthreads, T.piece, row, nbo);
+        if (ok && A.rows.cnt) ok = commit(A.rows, s, T.row_col, T.row_val, nthreads, row.cnt);
+        if (ok && A.nb.cnt) ok = commit(A.nb, s, T.nb_id, nullptr, nthreads, nbo.cnt);
+        if (!ok) {
+            if (next_list) {
+                const int k = atomicAdd(next_cnt, 1);
+                next_list[k] = int(s);
+            } else {
+                atomicOr(A.err, DE_CAPACITY);
+                if (A.mass) A.mass[s] = nan("");
+                if (A.rows.cnt) A.rows.cnt[s] = 0;
+                if (A.nb.cnt) A.nb.cnt[s] = 0;
+            }
+        }
+    }
+}
+
+template <int MODE, bool BALL>
+void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
+    constexpr int CAP = CAP_FAST_2D;
+    const size_t smem = size_t(CAP) * T2D * 16 + size_t(CAP * T2D + 1) / 2 * 8 +
+                        size_t(smem_extra_halves<MODE>()) * CAP * T2D * 4;
+    static bool attr_set = false;
+    if (!attr_set) {
+        SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        attr_set = true;
+    }
+    k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
+    SDOT_CUDA(cudaGetLastError());
+    double *scr = static_cast<double *>(scratch);
+    k_cells2d_tier<MODE, BALL, CAP_BIG_2D><<<ceil_div(BIG_THREADS, 64), 64, 0, st>>>(
+        a, scr, BIG_THREADS, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2);
+    SDOT_CUDA(cudaGetLastError());
+    k_cells2d_tier<MODE, BALL, CAP_HUGE_2D><<<ceil_div(HUGE_THREADS, 64), 64, 0, st>>>(
+        a, scr, HUGE_THREADS, a.ovf_list2, a.ovf_cnt2, nullptr, nullptr);
+    SDOT_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+size_t cells2d_scratch_bytes() {
+    const long long a = tier_doubles(BIG_THREADS, CAP_BIG_2D), b = tier_doubles(HUGE_THREADS, CAP_HUGE_2D);
+    return size_t(a > b ? a : b) * sizeof(double) + 256;
+}
+
+void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
+    if (a.n == 0) return;
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt2, 0, sizeof(int), st));
+    if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
+    if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
+    const bool ball = a.ball != 0;
+    if (a.mode == DM_SINGLE) {
+        if (ball) launch_all<DM_SINGLE, true>(a, scratch, st); else launch_all<DM_SINGLE, false>(a, scratch, st);
+    } else if (a.mode == DM_IMAGE) {
+        if (ball) launch_all<DM_IMAGE, true>(a, scratch, st); else launch_all<DM_IMAGE, false>(a, scratch, st);
+    } else {
+        if (ball) launch_all<DM_MULTI, true>(a, scratch, st); else launch_all<DM_MULTI, false>(a, scratch, st);
+    }
+}
+
+}  // namespace sdot

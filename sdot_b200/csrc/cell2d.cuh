@@ -1,0 +1,84 @@
+// 2D Laguerre-cell kernels: traversal + clipping + integrals + Hessian rows.
+#pragma once
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace sdot {
+
+enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2 };
+
+// Cell polygon capacities of the three tiers.  Every cell is first built by
+// the fast kernel (polygon in shared memory); cells that overflow it are
+// rebuilt by the big tier, then by the huge tier (polygons in global scratch).
+// Beyond the huge capacity the call reports ST_CAPACITY.
+constexpr int CAP_FAST_2D = 16;
+constexpr int CAP_BIG_2D = 64;
+constexpr int CAP_HUGE_2D = 1024;
+// Hessian rows and neighbour lists are stored slot-major (ELL) with these
+// widths; longer rows (only cells of the big / huge tiers) go to a side
+// buffer, their offset in row_side[s].
+constexpr int ROWCAP_2D = 24;
+constexpr int NBCAP_2D = 40;
+
+// Row storage shared by the cell kernels, the CSR assembly and the solver.
+struct Rows {
+    int *cnt = nullptr;        // entries per row (sorted order)
+    int *col = nullptr;        // ELL columns (sorted order)
+    double *val = nullptr;     // ELL values (may be null for id lists)
+    long long stride = 0;      // ELL slot stride (>= n)
+    int cap = 0;               // ELL width
+    long long *side = nullptr; // per row: offset in the side buffer when cnt > cap
+    int *side_col = nullptr;
+    double *side_val = nullptr;
+    long long side_cap = 0;
+    unsigned long long *side_used = nullptr;
+    __host__ __device__ int *colp(long long s, int k) const {
+        return cnt[s] > cap ? side_col + side[s] + k : col + k * stride + s;
+    }
+    __host__ __device__ double *valp(long long s, int k) const {
+        return cnt[s] > cap ? side_val + side[s] + k : val + k * stride + s;
+    }
+};
+
+struct Cell2DArgs {
+    long long n = 0;
+    const double *pos = nullptr;   // 2n, sorted order
+    const double *w = nullptr;     // n, sorted order
+    const TreeNode<2> *nodes = nullptr;
+    // starting polygon (single item polygon, inflated bbox, or image box)
+    int start_n = 0;
+    const double *start_xy = nullptr;  // 2 * start_n
+    double coeff = 1.0;                // single-item density
+    int mode = DM_SINGLE;
+    int ball = 0;
+    // image (nb_coeffs == 1)
+    double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};
+    int img_nx = 0, img_ny = 0;
+    const double *img = nullptr;
+    // multi items: item k has vertices [item_off[k], item_off[k+1]) in item_xy
+    // (2 per vertex) with outward unit normals item_nrm, density item_coeff[k]
+    int nitems = 0;
+    const int *item_off = nullptr;
+    const double *item_xy = nullptr;
+    const double *item_nrm = nullptr;
+    const double *item_coeff = nullptr;
+    // outputs (sorted order); null pointers skip that output
+    double *mass = nullptr;       // get_integrals
+    double *mass_c = nullptr;     // mass as get_centroids computes it
+    double *ctd = nullptr;        // 2n centroids
+    Rows rows;                    // Hessian rows (rows.cnt null: skipped)
+    Rows nb;                      // boundary ids of each cell (nb.cnt null: skipped)
+    // overflow handling (lists of sorted indices handed to the next tier)
+    int *ovf_list = nullptr;
+    int *ovf_cnt = nullptr;
+    int *ovf_list2 = nullptr;
+    int *ovf_cnt2 = nullptr;
+    unsigned *err = nullptr;
+};
+
+size_t cells2d_scratch_bytes();
+// Fast kernel over all cells, then the big and huge tiers over the overflow
+// lists.  `scratch` must hold cells2d_scratch_bytes() bytes.
+void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st);
+
+}  // namespace sdot

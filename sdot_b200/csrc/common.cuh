@@ -1,0 +1,76 @@
+// Shared definitions for the sdot_b200 CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+namespace sdot {
+
+// Status codes of the C ABI (mirrored in include/sdot_gpu.h).
+enum Status : int {
+    ST_OK = 0,
+    ST_VOID_CELL = 1,          // reference: for_each_laguerre_cell(stop_if_void) -> 1
+    ST_CAPACITY = 2,           // a cell needed more vertices than the fallback capacity
+    ST_NOT_CONVERGED = 3,
+    ST_ITER_CAP = 4,
+    ST_OOM = 5,
+    ST_BAD_ARG = 6,
+    ST_CUDA = 7,
+    ST_UNSUPPORTED = 8,
+};
+
+// Cut identifiers stored with each polygon edge (edge k joins vertex k and k+1).
+//  id >= 0            : the bisector with the Dirac at that SORTED position
+//  id == ID_ARC       : an arc of the clipping disc
+//  id <= ID_DOMAIN0   : edge (ID_DOMAIN0 - id) of the starting polygon (domain)
+constexpr int ID_ARC = -2;
+constexpr int ID_DOMAIN0 = -3;
+__host__ __device__ inline int domain_id(int e) { return ID_DOMAIN0 - e; }
+__host__ __device__ inline int domain_edge(int id) { return ID_DOMAIN0 - id; }
+
+// Inside a piece (cell intersected with a domain item or a pixel):
+//  id >= 0       : came from edge `id` of the cell polygon
+//  id == PID_OWN : an edge of the item/pixel itself
+//  id == ID_ARC  : an arc
+constexpr int PID_OWN = -1;
+
+struct CudaError {
+    cudaError_t err;
+    const char *where;
+};
+
+#define SDOT_CUDA(call)                                                         \
+    do {                                                                        \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess) throw ::sdot::CudaError{e_, #call};              \
+    } while (0)
+
+inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+// Per-cell kernel bodies are device functions; a host build of them (for
+// CPU-side debugging of the kernels) is compiled with SDOT_HOST_KERNELS.
+#ifdef SDOT_HOST_KERNELS
+#define SDOT_KFN __host__ __device__
+#else
+#define SDOT_KFN __device__
+#endif
+
+// Sets bits of the sticky error word (atomically on the device).
+__host__ __device__ inline void flag_error(unsigned *word, unsigned bits) {
+#ifdef __CUDA_ARCH__
+    atomicOr(word, bits);
+#else
+    *word |= bits;
+#endif
+}
+
+// Sticky per-context error word written by kernels (never __trap).
+enum DevErr : unsigned {
+    DE_CAPACITY = 1u,      // cell polygon overflowed its capacity (re-run in the large path)
+    DE_STACK = 2u,         // traversal stack overflow (should not happen: depth bounded)
+    DE_ITER = 4u,          // an iteration cap was reached
+    DE_PIECE = 8u,         // a piece overflowed its capacity
+};
+
+}  // namespace sdot

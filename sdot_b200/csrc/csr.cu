@@ -1,0 +1,124 @@
+// Hessian row assembly (see csr.cuh).
+#include "csr.cuh"
+
+namespace sdot {
+
+namespace {
+
+constexpr int TB = 256;
+
+// Merging never lengthens a row.  A side-buffer row whose merged count fits
+// the ELL width is moved to its ELL slots, so that Rows::colp (which picks
+// the storage from the count) stays consistent.
+__global__ void k_sort_merge(Rows R, long long n, const int *idx, long long *cnt_orig) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int m = R.cnt[s];
+    // insertion sort in place (rows are short: ~7 entries in 2D, ~16 in 3D)
+    for (int i = 1; i < m; ++i) {
+        const int c = *R.colp(s, i);
+        const double v = *R.valp(s, i);
+        const int oc = idx[c];
+        int j = i - 1;
+        while (j >= 0) {
+            const int cj = *R.colp(s, j);
+            const int ocj = idx[cj];
+            const double vj = *R.valp(s, j);
+            if (ocj < oc || (ocj == oc && !(vj > v))) break;
+            *R.colp(s, j + 1) = cj;
+            *R.valp(s, j + 1) = vj;
+            --j;
+        }
+        *R.colp(s, j + 1) = c;
+        *R.valp(s, j + 1) = v;
+    }
+    // merge equal columns
+    int o = 0;
+    for (int i = 0; i < m; ++i) {
+        const int c = *R.colp(s, i);
+        const double v = *R.valp(s, i);
+        if (i + 1 < m && *R.colp(s, i + 1) == c) {
+            *R.valp(s, i + 1) += v;
+            continue;
+        }
+        *R.colp(s, o) = c;
+        *R.valp(s, o) = v;
+        ++o;
+    }
+    if (m > R.cap && o <= R.cap) {
+        for (int k = 0; k < o; ++k) {
+            const int c = *R.colp(s, k);
+            const double v = *R.valp(s, k);
+            R.col[k * R.stride + s] = c;
+            R.val[k * R.stride + s] = v;
+        }
+    }
+    R.cnt[s] = o;
+    cnt_orig[idx[s]] = o;
+}
+
+__global__ void k_write(Rows R, long long n, const int *idx, const long long *offsets, long long *cols, double *vals) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int m = R.cnt[s];
+    const long long o = offsets[idx[s]];
+    for (int i = 0; i < m; ++i) {
+        cols[o + i] = idx[*R.colp(s, i)];
+        vals[o + i] = *R.valp(s, i);
+    }
+}
+
+__global__ void k_nb_counts(Rows NB, long long n, const int *idx, long long *cnt_orig) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    cnt_orig[idx[s]] = NB.cnt[s];
+}
+
+__global__ void k_nb_write(Rows NB, long long n, const int *idx, const long long *offsets, long long *ids) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int m = NB.cnt[s];
+    const long long o = offsets[idx[s]];
+    for (int i = 0; i < m; ++i) {
+        const int id = *NB.colp(s, i);
+        ids[o + i] = id >= 0 ? (long long)idx[id] : (id == ID_ARC ? -2 : -1);
+    }
+}
+
+__global__ void k_unpermute(const double *in, double *out, long long n, int d, const int *idx) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const long long i = idx[s];
+    for (int k = 0; k < d; ++k) out[i * d + k] = in[s * d + k];
+}
+
+}  // namespace
+
+void csr_sort_merge(const Rows &R, long long n, const int *idx, long long *cnt_orig, cudaStream_t st) {
+    if (n <= 0) return;
+    k_sort_merge<<<ceil_div(n, TB), TB, 0, st>>>(R, n, idx, cnt_orig);
+    SDOT_CUDA(cudaGetLastError());
+}
+void csr_write(const Rows &R, long long n, const int *idx, const long long *offsets, long long *cols, double *vals,
+               cudaStream_t st) {
+    if (n <= 0) return;
+    k_write<<<ceil_div(n, TB), TB, 0, st>>>(R, n, idx, offsets, cols, vals);
+    SDOT_CUDA(cudaGetLastError());
+}
+void nb_counts(const Rows &NB, long long n, const int *idx, long long *cnt_orig, cudaStream_t st) {
+    if (n <= 0) return;
+    k_nb_counts<<<ceil_div(n, TB), TB, 0, st>>>(NB, n, idx, cnt_orig);
+    SDOT_CUDA(cudaGetLastError());
+}
+void nb_write(const Rows &NB, long long n, const int *idx, const long long *offsets, long long *ids, cudaStream_t st) {
+    if (n <= 0) return;
+    k_nb_write<<<ceil_div(n, TB), TB, 0, st>>>(NB, n, idx, offsets, ids);
+    SDOT_CUDA(cudaGetLastError());
+}
+void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st) {
+    if (n <= 0) return;
+    k_unpermute<<<ceil_div(n, TB), TB, 0, st>>>(in, out, n, d, idx);
+    SDOT_CUDA(cudaGetLastError());
+}
+
+}  // namespace sdot

@@ -1,0 +1,23 @@
+// Hessian row assembly: rows in sorted (Morton) order -> reference CSR.
+#pragma once
+#include "cell2d.cuh"
+#include "common.cuh"
+
+namespace sdot {
+
+// Sort each row by (original column, value) and merge equal columns the way
+// get_der_integrals_wrt_weights does (get_der_integrals_wrt_weights.h:76-88):
+// values of equal columns are summed in ascending value order.  Rewrites the
+// rows in place and stores the merged count both in R.cnt[s] (rows keep
+// their storage) and in cnt_orig[idx[s]] (original order, for the scan).
+void csr_sort_merge(const Rows &R, long long n, const int *idx, long long *cnt_orig, cudaStream_t st);
+// Write rows to CSR in original order: columns as original indices (int64).
+void csr_write(const Rows &R, long long n, const int *idx, const long long *offsets, long long *cols, double *vals,
+               cudaStream_t st);
+// Neighbour lists: ids mapped (sorted -> original; domain edges -> -1; arcs -> -2).
+void nb_counts(const Rows &NB, long long n, const int *idx, long long *cnt_orig, cudaStream_t st);
+void nb_write(const Rows &NB, long long n, const int *idx, const long long *offsets, long long *ids, cudaStream_t st);
+// out[idx[s] * d + k] = in[s * d + k]
+void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st);
+
+}  // namespace sdot

@@ -1,0 +1,170 @@
+"""GPU (CUDA, sm_100a) vs the compiled reference oracle, 2D, FP64.
+
+Tolerances.  A clipped cell's rounding error is absolute (set by the size of
+its coordinates, not of the cell), so each quantity's error is measured
+against max(|reference value|, the mean of that quantity over all cells):
+  masses     |m_gpu - m_ref|     <= RTOL * max(|m_ref|, mean mass)
+  centroids  |c_gpu - c_ref|     <= RTOL * max(|c_ref|, 1)         (unit-size domains)
+  Hessian    |H_gpu - H_ref|     <= RTOL * max(|H_ref|, mean |H_ii|)
+with RTOL = 1e-12, except where a test states a larger value and why.
+Neighbour sets and the CSR sparsity pattern must match exactly on these
+non-degenerate inputs.
+"""
+import numpy as np
+import pytest
+
+from sdot_b200 import workloads
+from tests.helpers import assert_close, compare_csr, make_pair, neighbor_sets
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def check_all(gpu, ref, n, rtol=RTOL, rtol_hess=None, check_nb=True):
+    rtol_hess = rtol if rtol_hess is None else rtol_hess
+    m_r = ref.integrals()
+    mean = max(float(np.abs(m_r).mean()), 1e-300)
+    m_g = gpu.integrals()
+    assert_close(m_g, m_r, rtol, mean, "masses")
+    c_g, mc_g = gpu.centroids(with_masses=True)
+    c_r, mc_r = ref.centroids(with_masses=True)
+    assert_close(mc_g, mc_r, rtol, mean, "centroid masses")
+    assert_close(c_g, c_r, rtol, 1.0, "centroids")
+    off, col, val, mas = gpu.der_integrals_wrt_weights()
+    err, ro, rc, rv, rm = ref.der_integrals_wrt_weights()
+    assert err == 0
+    assert_close(mas, rm, rtol, mean, "der masses")
+    diag = np.zeros(n)
+    rows = np.repeat(np.arange(n), np.diff(ro))
+    sel = rc == rows
+    diag[rows[sel]] = np.abs(rv[sel])
+    compare_csr((off, col, val), (ro, rc, rv), rtol_hess, max(diag.mean(), 1e-300))
+    if check_nb:
+        go, gi = gpu.neighbors()
+        ro2, ri = ref.neighbors()
+        gs, rs = neighbor_sets(go, gi), neighbor_sets(ro2, ri)
+        bad = [i for i in range(n) if gs[i] != rs[i]]
+        assert not bad, f"{len(bad)} neighbour sets differ, first {bad[:5]}: {gs[bad[0]]} vs {rs[bad[0]]}"
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 100, 2000])
+def test_uniform_unit_box(gpu_lib, ref_oracle, n):
+    rng = np.random.default_rng(100 + n)
+    p = rng.random((n, 2))
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle)
+    check_all(gpu, ref, n)
+
+
+def test_config1_full_size(gpu_lib, ref_oracle):
+    c = workloads.config1()
+    n = len(c["weights"])
+    gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle)
+    check_all(gpu, ref, n)
+    assert abs(gpu.integrals().sum() - 1.0) < 1e-12
+
+
+def test_clustered_with_weights(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(7)
+    n = 20000
+    p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng)])
+    w = rng.uniform(-1e-6, 1e-6, n) * 1e-2
+    gpu, ref = make_pair(p, w, ref_oracle)
+    check_all(gpu, ref, n)
+
+
+def test_config2_weights_void_cells(gpu_lib, ref_oracle):
+    # C2's weight spread (U[-1e-6, 1e-6]) on clustered points: ~40% void cells
+    # and sliver cells whose edges are set by weight differences 1e4 times the
+    # squared spacing; the two CPU oracles (reference and restatement) differ
+    # by 1.5e-12 of the mean diagonal there, so the Hessian bound is 1e-11.
+    c = workloads.config2(n=50_000)
+    gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle)
+    m = gpu.integrals()
+    assert (m == 0).sum() > 0
+    check_all(gpu, ref, 50_000, rtol_hess=1e-11)
+
+
+def test_voronoi_boundary_clamped_points(gpu_lib, ref_oracle):
+    # clustered points clamped to the box: long collinear runs on the box
+    # edges give cells with hundreds of vertices (the large-capacity tiers)
+    c = workloads.config2(n=100_000)
+    gpu, ref = make_pair(c["positions"], np.zeros(100_000), ref_oracle)
+    check_all(gpu, ref, 100_000)
+    assert gpu.last_overflow_count() > 0
+
+
+def test_disc_clip_box(gpu_lib, ref_oracle):
+    # arcs use atan2 / sin / cos, whose device and host libm results differ
+    # by a few ulp: masses and Hessian within 1e-11
+    rng = np.random.default_rng(3)
+    n = 3000
+    p = rng.random((n, 2))
+    w = np.full(n, (0.5 / np.sqrt(n)) ** 2) * rng.uniform(0.5, 2.0, n)
+    gpu, ref = make_pair(p, w, ref_oracle, radial_func="in_ball_w05")
+    check_all(gpu, ref, n, rtol=1e-11)
+
+
+def test_image_density(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(4)
+    n = 3000
+    p = rng.random((n, 2))
+    img = workloads.c3_image(res=64)
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, image=img)
+    check_all(gpu, ref, n)
+    assert abs(gpu.integrals().sum() - 0.8) < 1e-11
+
+
+def test_image_density_disc_clip(gpu_lib, ref_oracle):
+    c = workloads.config3(n=5000, res=128)
+    gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle, radial_func="in_ball_w05", image=c["image"])
+    check_all(gpu, ref, 5000, rtol=1e-11)
+
+
+def test_multi_items(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(5)
+    n = 2000
+    p = rng.random((n, 2)) * [2.0, 1.0]
+    shapes = [("add_box_shape", ([0.0, 0.0], [1.0, 1.0], 1.0)),
+              ("add_box_shape", ([1.0, 0.0], [2.0, 1.0], 0.5)),
+              ("add_simplex_shape", ([[0.2, 0.2], [0.9, 0.3], [0.4, 0.8]], 2.0))]
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, shapes=shapes)
+    check_all(gpu, ref, n)
+
+
+def test_multi_items_disc_clip(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(8)
+    n = 1500
+    p = rng.random((n, 2)) * [2.0, 1.0]
+    w = np.full(n, 0.3 / n) * rng.uniform(0.5, 2.0, n)
+    shapes = [("add_box_shape", ([0.0, 0.0], [1.0, 1.0], 1.0)),
+              ("add_box_shape", ([1.0, 0.0], [2.0, 1.0], 0.5))]
+    gpu, ref = make_pair(p, w, ref_oracle, radial_func="in_ball_w05", shapes=shapes)
+    check_all(gpu, ref, n, rtol=1e-11)
+
+
+def test_convex_polyhedron_domain(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(6)
+    n = 2000
+    ang = np.linspace(0, 2 * np.pi, 7)[:-1]
+    pts = np.stack([0.5 + 0.5 * np.cos(ang), 0.5 + 0.5 * np.sin(ang)], 1)
+    nrm = np.stack([np.cos(ang), np.sin(ang)], 1)
+    p = 0.5 + (rng.random((n, 2)) - 0.5) * 0.8
+    shapes = [("add_convex_polyhedron_shape", (pts, nrm, 1.0))]
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, shapes=shapes)
+    check_all(gpu, ref, n)
+
+
+def test_deterministic_repeat(gpu_lib):
+    # per-row ownership: two evaluations give bitwise identical results
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config2(n=200_000)
+    outs = []
+    for _ in range(2):
+        g = PowerDiagram(c["positions"], c["weights"])
+        g.add_box_shape([0, 0], [1, 1])
+        outs.append((g.integrals(), g.der_integrals_wrt_weights()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    for a, b in zip(outs[0][1], outs[1][1]):
+        assert np.array_equal(a, b)
