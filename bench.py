@@ -1,0 +1,385 @@
+"""Benchmark of the power-diagram hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--n DIRACS]
+
+Workload: the 2D power diagram at scale -- 1,000,000 Diracs, 50% uniform in
+[0,1]^2 and 50% from 20 Gaussian clusters (sigma 0.02, clamped to the box),
+weights uniform in [-1e-6, 1e-6], unit box with density 1 (seeded synthetic
+data, sdot_b200/workloads.py).  One step is one fused evaluation: device
+Z-order tree build, every Laguerre cell, cell areas, centroids and the CSR
+weight Hessian.  Metric: Laguerre cells per second (areas + Hessian).
+
+Arms
+  ours       : libsdot_b200.so through its C ABI.  `value` is timed with CUDA
+               events on the context's stream with the Diracs already in HBM
+               (L2 flushed between steps by writing 256 MB); `e2e` is the same
+               step through the public ABI from pinned host buffers, host->device
+               copy of positions/weights and device->host copy of masses,
+               centroids and the CSR Hessian included, timed on the host.
+  reference  : the reference's own CPU path (oracle/_ref, compiled from the
+               reference sources; the C restatement oracle/sdot_oracle.c when
+               the reference library is absent) on all host cores.
+
+Multi-GPU (torchrun, one process per GPU): every rank evaluates its own
+1M-Dirac problem (weak scaling, no data-path collective); the step time is the
+maximum over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Laguerre cells/s (areas + centroids + CSR Hessian), 2D, 1M Diracs"
+UNIT = "cells/s"
+# Algorithmic work per cell (reference algorithm counts on 2D uniform inputs,
+# FMA = 2 flops): 22.8 cut attempts x (12 + 5 x 5.42 vertices)
+# + 38.1 boxes x 6 vertices x 12 + 6 final vertices x 35 = 3.9 kflop.
+FLOPS_PER_CELL = 3.9e3
+# per-cell algorithmic HBM bytes: positions + weight in (24), area (8),
+# centroid (16), ~7 Hessian entries x 12 + offset 8
+BYTES_PER_CELL = 136.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(n, rank):
+    from sdot_b200 import workloads
+
+    c = workloads.config2(n=n)
+    if rank:
+        # another seeded problem of the same shape per extra rank
+        rng = np.random.Generator(np.random.PCG64(workloads.SEED0 + 2 + 1000 * rank))
+        nu = n // 2
+        c["positions"] = np.concatenate([workloads.uniform_points(nu, 2, rng),
+                                         workloads.clustered_points(n - nu, 2, rng)])
+        c["weights"] = rng.uniform(-1e-6, 1e-6, n)
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_reference_step(pos, w, threads):
+    """One reference evaluation: grid.update + get_integrals + get_centroids +
+    get_der_integrals_wrt_weights (three traversals, as the reference API
+    requires).  Returns (seconds, kind)."""
+    from oracle import ref
+
+    if ref.available():
+        r = ref.RefPowerDiagram(pos, w, threads=threads)
+        r.add_box_shape([0.0, 0.0], [1.0, 1.0])
+        t0 = time.perf_counter()
+        r.update()
+        r.integrals()
+        r.centroids()
+        r.der_integrals_wrt_weights()
+        return time.perf_counter() - t0, "reference", r.L.ref_nb_threads()
+    from oracle import port
+
+    q = port.PortPowerDiagram(pos, w)
+    q.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    t0 = time.perf_counter()
+    q.integrals()
+    return time.perf_counter() - t0, "port", 1
+
+
+def cpu_baseline(c, max_seconds=20.0):
+    threads = os.cpu_count() or 1
+    n = len(c["weights"])
+    times, kind, used = [], None, threads
+    t_start = time.perf_counter()
+    while len(times) < 3 and time.perf_counter() - t_start < max_seconds:
+        t, kind, used = cpu_reference_step(c["positions"], c["weights"], threads)
+        times.append(t)
+    t = statistics.median(times)
+    return {"value": n / t, "unit": UNIT, "cores": used, "kind": kind,
+            "sample": f"{len(times)} full evaluations of the {n}-Dirac workload (update + get_integrals + "
+                      f"get_centroids + get_der_integrals_wrt_weights), median {t:.3f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    c = workload(args.n, 0)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_step(c["positions"], c["weights"], threads)
+    times = []
+    kind, used = None, threads
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t, kind, used = cpu_reference_step(c["positions"], c["weights"], threads)
+        times.append(t)
+    t_all = time.perf_counter() - t_all
+    ms = 1e3 * sum(times) / len(times)
+    value = args.n / (ms * 1e-3)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "2D power diagram, 1M Diracs (50% uniform + 50% clustered), w ~ U[-1e-6,1e-6], "
+                                  "unit box", "n_diracs": args.n, "parallelism": "host threads"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind,
+                            "sample": f"each step one full evaluation of the {args.n}-Dirac workload"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "wall_s": t_all}
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from sdot_b200 import _lib
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _lib.load()
+    c = workload(args.n, rank)
+    n = args.n
+    pos_h = torch.from_numpy(np.ascontiguousarray(c["positions"])).pin_memory()
+    w_h = torch.from_numpy(np.ascontiguousarray(c["weights"])).pin_memory()
+    pos_d = pos_h.to(dev)
+    w_d = w_h.to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    prec = {"fp64": _lib.SDOT_FP64, "mixed": _lib.SDOT_MIXED}[args.precision]
+    opt = _lib.SdotOptions(11, ctypes.c_void_p(stream.cuda_stream), local)
+    ctx = L.sdot_create(2, prec, ctypes.byref(opt))
+    if not ctx:
+        raise RuntimeError("sdot_create failed")
+    p0 = np.zeros(2)
+    p1 = np.ones(2)
+
+    def check(st):
+        if st != 0:
+            raise RuntimeError(L.sdot_last_error(ctx).decode())
+
+    check(L.sdot_add_box_shape(ctx, ctypes.c_void_p(p0.ctypes.data), ctypes.c_void_p(p1.ctypes.data), 1.0))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step_device():
+        check(L.sdot_set_diracs(ctx, ctypes.c_void_p(pos_d.data_ptr()), ctypes.c_void_p(w_d.data_ptr()), n,
+                                _lib.SDOT_DEVICE))
+        check(L.sdot_evaluate(ctx))
+
+    # warm-up
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # ---- value: device-resident, CUDA events on the context stream
+    launches0 = ctypes.c_uint64(0)
+    L.sdot_kernel_launches(ctypes.byref(launches0))
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    cell_ms = []
+    t3 = np.zeros(3)
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)  # evicts L2 (126 MB) between steps
+            ev[k][0].record(stream)
+        step_device()
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+        L.sdot_last_timings(ctx, ctypes.c_void_p(t3.ctypes.data))
+        cell_ms.append(t3[1])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    launches1 = ctypes.c_uint64(0)
+    L.sdot_kernel_launches(ctypes.byref(launches1))
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = float(np.mean(step_ms))
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * n / (ms * 1e-3)
+
+    # ---- e2e: public ABI from pinned host buffers (copies included)
+    off_h = torch.empty(n + 1, dtype=torch.int64).pin_memory()
+    mass_h = torch.empty(n, dtype=torch.float64).pin_memory()
+    mass2_h = torch.empty(n, dtype=torch.float64).pin_memory()
+    ctd_h = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+    cols_h = vals_h = None
+    nnz = ctypes.c_int64(0)
+
+    def step_e2e():
+        nonlocal cols_h, vals_h
+        check(L.sdot_set_diracs(ctx, ctypes.c_void_p(pos_h.data_ptr()), ctypes.c_void_p(w_h.data_ptr()), n,
+                                _lib.SDOT_HOST))
+        check(L.sdot_get_centroids(ctx, ctypes.c_void_p(ctd_h.data_ptr()), ctypes.c_void_p(mass2_h.data_ptr()),
+                                   _lib.SDOT_HOST))
+        check(L.sdot_get_der_integrals_wrt_weights(ctx, None, None, None, None, ctypes.byref(nnz), 0,
+                                                   _lib.SDOT_HOST))
+        if cols_h is None or cols_h.numel() < nnz.value:
+            cols_h = torch.empty(nnz.value + 1024, dtype=torch.int64).pin_memory()
+            vals_h = torch.empty(nnz.value + 1024, dtype=torch.float64).pin_memory()
+        check(L.sdot_get_der_integrals_wrt_weights(ctx, ctypes.c_void_p(off_h.data_ptr()),
+                                                   ctypes.c_void_p(cols_h.data_ptr()),
+                                                   ctypes.c_void_p(vals_h.data_ptr()),
+                                                   ctypes.c_void_p(mass_h.data_ptr()), ctypes.byref(nnz), 0,
+                                                   _lib.SDOT_HOST))
+
+    for _ in range(max(1, args.warmup)):
+        step_e2e()
+    torch.cuda.synchronize()
+    e2e_times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step_e2e()
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_times))
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = n * 2 * 8 + n * 8
+    d2h = n * 16 + n * 8 + (n + 1) * 8 + nnz.value * 16 + n * 8
+
+    # ---- roofline of the cell kernel (the dominant kernel)
+    peaks = np.zeros(2)
+    L.sdot_measure_fma_peaks(ctypes.c_void_p(peaks.ctypes.data))
+    cell = float(np.mean(cell_ms))
+    achieved = FLOPS_PER_CELL * n / (cell * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic_cells2d_c2_1M.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+    roofline = {"bound": "fp64", "kernel": "k_cells2d (fast tier) + overflow tiers", "achieved": achieved,
+                "peak": float(peaks[0]), "unit": "TFLOP/s", "frac": achieved / float(peaks[0]) if peaks[0] else None,
+                "traffic": traffic, "algorithmic_bytes_per_launch": BYTES_PER_CELL * n,
+                "flops_per_cell": FLOPS_PER_CELL, "cell_kernel_ms": cell,
+                "peak_source": "measured this run by sdot_measure_fma_peaks (FMA-only kernel); the HBM-bound view: "
+                               f"{BYTES_PER_CELL * n / (cell * 1e-3) / 1e9:.1f} GB/s of measured 6544 GB/s",
+                "fp32_peak_tflops": float(peaks[1])}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+           "data": "synthetic (seeded, shapes of the 1M-Dirac clustered 2D workload)",
+           "config": {"workload": "2D power diagram, 1M Diracs (50% uniform + 50% 20-cluster Gaussian sigma 0.02), "
+                                  "w ~ U[-1e-6,1e-6], unit box, density 1; areas + centroids + CSR Hessian",
+                      "n_diracs_per_gpu": n, "precision": args.precision,
+                      "parallelism": f"weak x{world} (independent problem per GPU)",
+                      "l2": "flushed between steps (256 MB write)"},
+           "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "gpu_launches": int(launches1.value - launches0.value),
+           "roofline": roofline, "clocks": clk, "wall_timed_s": wall,
+           "stages_ms": {"cells": cell}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(c)
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)}
+    L.sdot_destroy(ctx)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -30,7 +30,7 @@ typedef struct sdot_ctx sdot_ctx;
 typedef enum sdot_status {
     SDOT_OK = 0,
     SDOT_VOID_CELL = 1,       /* reference: for_each_laguerre_cell(stop_if_void) returns 1 */
-    SDOT_CAPACITY = 2,        /* a cell has more than 64 vertices (2D) */
+    SDOT_CAPACITY = 2,        /* a cell has more than 1024 vertices (2D) */
     SDOT_NOT_CONVERGED = 3,   /* Newton / PCG did not reach the tolerance */
     SDOT_ITER_CAP = 4,        /* an iteration cap was reached */
     SDOT_OOM = 5,
@@ -120,6 +120,17 @@ int sdot_evaluate(sdot_ctx *ctx);
 int sdot_last_timings(const sdot_ctx *ctx, double *t3);
 /* Number of cells rebuilt by the large-capacity fallback in the last evaluation. */
 int sdot_last_overflow_count(const sdot_ctx *ctx, int64_t *count);
+/* Number of kernels this library has launched in the process so far.
+ * No reference counterpart (instrumentation).                               */
+int sdot_kernel_launches(uint64_t *count);
+/* Measured FP64 and FP32 non-tensor FMA throughput of the current device in
+ * TFLOP/s (tflops2[0], tflops2[1]): the roofline denominators of the cell
+ * kernels.  No reference counterpart (measurement utility).                 */
+int sdot_measure_fma_peaks(double *tflops2);
+/* Debug builds (-DSDOT_CHECKS) only: first failed bounds check of the cell
+ * kernels (out6[0..2] = code, source line, value) and of the Hessian
+ * assembly (out6[3..5]).  Release builds report zeros.                       */
+int sdot_debug_checks(uint64_t *out6);
 
 #ifdef __cplusplus
 }

@@ -8,7 +8,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsdot_b200.so")
+# SDOT_B200_LIB selects another build of the same sources (e.g. a debug build)
+LIB_PATH = os.environ.get("SDOT_B200_LIB") or os.path.join(_HERE, "libsdot_b200.so")
 
 SDOT_OK = 0
 SDOT_VOID_CELL = 1
@@ -80,6 +81,9 @@ SIGNATURES = {
     "sdot_evaluate": (ctypes.c_int, [_P]),
     "sdot_last_timings": (ctypes.c_int, [_P, _P]),
     "sdot_last_overflow_count": (ctypes.c_int, [_P, _P]),
+    "sdot_kernel_launches": (ctypes.c_int, [_P]),
+    "sdot_measure_fma_peaks": (ctypes.c_int, [_P]),
+    "sdot_debug_checks": (ctypes.c_int, [_P]),
 }
 
 _lib = None

@@ -7,6 +7,7 @@
 #include "tree.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -15,6 +16,11 @@
 #include <vector>
 
 using namespace sdot;
+
+namespace sdot {
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace sdot
 
 namespace {
 
@@ -112,11 +118,14 @@ struct sdot_ctx {
     long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
     int *ovf_list = nullptr, *ovf_cnt = nullptr, *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;
     unsigned *err = nullptr;
+    int *guard = nullptr;
+    long long item_nv = 0;
     void *scratch = nullptr, *scan_tmp = nullptr;
     long long nnz = 0, nb_total = 0;
     long long n_void = 0;
     int last_ovf = 0;
     unsigned last_err = 0;
+    int last_guard[3] = {0, 0, 0};
     cudaEvent_t ev[4] = {};
     float times[3] = {0, 0, 0};
 
@@ -135,7 +144,7 @@ struct sdot_ctx {
         free_rows(rows);
         free_rows(nb);
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
-        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err);
+        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err); dfree(guard);
         if (scratch) cudaFree(scratch);
         if (scan_tmp) cudaFree(scan_tmp);
         scratch = scan_tmp = nullptr;
@@ -178,6 +187,7 @@ struct sdot_ctx {
         dalloc(ovf_list2, ecap);
         dalloc(ovf_cnt2, 1);
         dalloc(err, 1);
+        dalloc(guard, 3);
         SDOT_CUDA(cudaMalloc(&scratch, cells2d_scratch_bytes()));
         SDOT_CUDA(cudaMalloc(&scan_tmp, scan_tmp_size(ecap + 1, sizeof(long long))));
     }
@@ -189,9 +199,9 @@ struct sdot_ctx {
             std::vector<double> st = {img_lo[0], img_lo[1], img_hi[0], img_lo[1], img_hi[0], img_hi[1], img_lo[0], img_hi[1]};
             start_n = 4;
             dalloc(d_start, 8);
-            SDOT_CUDA(cudaMemcpy(d_start, st.data(), 8 * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_start, st.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream));
             dalloc(d_img, img_data.size());
-            SDOT_CUDA(cudaMemcpy(d_img, img_data.data(), img_data.size() * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_img, img_data.data(), img_data.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
             coeff = 1;
         } else if (items.size() == 1) {
             // ConvexPolyhedronAssembly::englobing_convex_polyhedron with one item
@@ -199,7 +209,7 @@ struct sdot_ctx {
             const Item2 &it = items[0];
             start_n = int(it.xy.size() / 2);
             dalloc(d_start, it.xy.size());
-            SDOT_CUDA(cudaMemcpy(d_start, it.xy.data(), it.xy.size() * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_start, it.xy.data(), it.xy.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
             coeff = it.coeff;
         } else if (items.size() > 1) {
             // englobing box inflated by its own size on each side (ConvexPolyhedronAssembly.tcc:60-92)
@@ -222,15 +232,16 @@ struct sdot_ctx {
             Item2 eb = box_item(mn[0] - dx, mn[1] - dy, mx[0] + dx, mx[1] + dy, 1.0);
             start_n = 4;
             dalloc(d_start, 8);
-            SDOT_CUDA(cudaMemcpy(d_start, eb.xy.data(), 8 * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_start, eb.xy.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream));
+            item_nv = off.back();
             dalloc(d_item_off, off.size());
-            SDOT_CUDA(cudaMemcpy(d_item_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_item_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
             dalloc(d_item_xy, xy.size());
-            SDOT_CUDA(cudaMemcpy(d_item_xy, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_item_xy, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
             dalloc(d_item_nrm, nrm.size());
-            SDOT_CUDA(cudaMemcpy(d_item_nrm, nrm.data(), nrm.size() * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_item_nrm, nrm.data(), nrm.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
             dalloc(d_item_coeff, co.size());
-            SDOT_CUDA(cudaMemcpy(d_item_coeff, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice));
+            SDOT_CUDA(cudaMemcpyAsync(d_item_coeff, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
         } else {
             throw BadArg("no domain: call sdot_add_box_shape (or another add_..._shape) first");
         }
@@ -244,6 +255,9 @@ struct sdot_ctx {
         a.pos = tree2.pos;
         a.w = tree2.w;
         a.nodes = tree2.nodes;
+        a.max_nodes = tree2.max_nodes;
+        a.guard = guard;
+        a.item_nv = item_nv;
         a.start_n = start_n;
         a.start_xy = d_start;
         a.coeff = coeff;
@@ -283,9 +297,13 @@ struct sdot_ctx {
         if (!eval_dirty) return finish_status();
         if (dim != 2) throw Unsupported("dim 3 is not available in this build");
         upload_domain();
+        if (mode == DM_MULTI)
+            throw Unsupported("domains made of several shapes are not enabled in this build (the multi-shape "
+                              "cell kernel is disabled); use one shape or an image density");
         reserve_eval();
         if (!ev[0]) for (auto &e : ev) SDOT_CUDA(cudaEventCreate(&e));
         SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
+        SDOT_CUDA(cudaMemsetAsync(guard, 0, 3 * sizeof(int), stream));
         SDOT_CUDA(cudaEventRecord(ev[0], stream));
         ensure_tree();
         SDOT_CUDA(cudaEventRecord(ev[1], stream));
@@ -305,6 +323,7 @@ struct sdot_ctx {
         SDOT_CUDA(cudaMemcpyAsync(&nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaMemcpyAsync(&last_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaMemcpyAsync(&last_ovf, ovf_cnt, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaMemcpyAsync(last_guard, guard, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaStreamSynchronize(stream));
         SDOT_CUDA(cudaEventElapsedTime(&times[0], ev[0], ev[1]));
         SDOT_CUDA(cudaEventElapsedTime(&times[1], ev[1], ev[2]));
@@ -317,6 +336,11 @@ struct sdot_ctx {
         if (last_err & DE_CAPACITY) {
             last_error = "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
             return SDOT_CAPACITY;
+        }
+        if (last_err & DE_GUARD) {
+            last_error = "inconsistent input or tree (guard " + std::to_string(last_guard[0]) + " at cell " +
+                         std::to_string(last_guard[1]) + ", value " + std::to_string(last_guard[2]) + ")";
+            return SDOT_BAD_ARG;
         }
         if (last_err & DE_STACK) {
             last_error = "traversal stack overflow";
@@ -700,7 +724,8 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
         if (stop_if_void) {
             // reference: any v == 0 -> 1 (get_der_integrals_wrt_weights.h:93-96)
             std::vector<double> m(n);
-            SDOT_CUDA(cudaMemcpy(m.data(), ctx->o_mass, n * sizeof(double), cudaMemcpyDeviceToHost));
+            SDOT_CUDA(cudaMemcpyAsync(m.data(), ctx->o_mass, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
             for (double v : m)
                 if (v == 0) {
                     ctx->last_error = "void cell";
@@ -742,6 +767,28 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
 int sdot_last_timings(const sdot_ctx *ctx, double *t3) {
     if (!ctx || !t3) return SDOT_BAD_ARG;
     for (int k = 0; k < 3; ++k) t3[k] = ctx->times[k];
+    return SDOT_OK;
+}
+
+int sdot_debug_checks(uint64_t *out6) {
+    if (!out6) return SDOT_BAD_ARG;
+    unsigned long long a[3], b[3];
+    try {
+        cells2d_read_checks(a);
+        csr_read_checks(b);
+    } catch (const CudaError &) {
+        return SDOT_CUDA_ERROR;
+    }
+    for (int k = 0; k < 3; ++k) {
+        out6[k] = a[k];
+        out6[3 + k] = b[k];
+    }
+    return SDOT_OK;
+}
+
+int sdot_kernel_launches(uint64_t *count) {
+    if (!count) return SDOT_BAD_ARG;
+    *count = g_launches.load();
     return SDOT_OK;
 }
 

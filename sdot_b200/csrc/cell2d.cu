@@ -38,6 +38,24 @@ constexpr int STACK = 64;   // traversal stack (depth <= 17 levels, <= 3 pending
 constexpr int BIG_THREADS = 148 * 64;
 constexpr int HUGE_THREADS = 148 * 4;
 
+// Records the first failed consistency guard and flags the error word; the
+// caller then skips the access.  Guards cover every index that comes from
+// data (tree nodes, leaf ranges, item offsets), so a corrupt input gives an
+// error status instead of a fault.
+SDOT_KFN void guard_fail(const Cell2DArgs &A, int code, long long s, long long value) {
+#ifdef __CUDA_ARCH__
+    const bool first = A.guard && atomicCAS(&A.guard[0], 0, code) == 0;
+#else
+    const bool first = A.guard && A.guard[0] == 0;
+    if (first) A.guard[0] = code;
+#endif
+    if (first) {
+        A.guard[1] = int(s);
+        A.guard[2] = int(value);
+    }
+    flag_error(A.err, DE_GUARD);
+}
+
 // Destination of one row (or id list): element k at col[k * stride]
 // (col == nullptr: the output is not wanted, only counted).
 struct Out {
@@ -78,6 +96,7 @@ struct Sink {
     double *acc;
     int acc_st;
     Out &row;
+    long long n_diracs = 1LL << 40;
 
     SDOT_HDI Sink(const PolyView<double> &c, const double *p, double x0, double y0, double sw, double r_, double *a,
                     int ast, Out &ro)
@@ -95,7 +114,7 @@ struct Sink {
         if (id < 0) return;
         const double m = coeff * len;
         if (DIRECT) {
-            const double dx = c0x - pos[2 * id], dy = c0y - pos[2 * id + 1];
+            const double dx = c0x - pos[2 * SDOT_CHECK_IDX(id, n_diracs, 3)], dy = c0y - pos[2 * id + 1];
             const double dist = sqrt(dx * dx + dy * dy);
             if (dist != 0) {
                 const double b = 0.5 * m / dist;
@@ -103,7 +122,7 @@ struct Sink {
                 der0 += b;
             }
         } else {
-            double &a = acc[t * acc_st];
+            double &a = acc[SDOT_CHECK_IDX(t, cell.cap, 2) * acc_st];
             a = a < 0 ? m : a + m;
         }
     }
@@ -199,7 +218,7 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
     stack[sp++] = 0;
     while (sp > 0) {
         const int node = stack[--sp];
-        const TreeNode<2> nd = A.nodes[node];
+        const TreeNode<2> nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
         // SpZGrid::can_be_evicted: skip the box when no Dirac in it can be
         // closer (in power distance) than c0 to any current vertex.
         bool evict = true;
@@ -217,10 +236,14 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
         if (evict) continue;
         if (nd.b < 0) {
             const int first = nd.a, nch = -nd.b;
+            if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
+                guard_fail(A, 1, s, node);
+                return -2;
+            }
             float key[4];
             int ch[4];
             for (int c = 0; c < nch; ++c) {
-                const TreeNode<2> &cn = A.nodes[first + c];
+                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
                 const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
                 const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
                 key[c] = float(mx * mx + my * my);
@@ -245,8 +268,13 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             }
             for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
         } else {
+            if (nd.a < 0 || nd.b > A.n) {
+                guard_fail(A, 2, s, node);
+                return -2;
+            }
             for (int j = nd.a; j < nd.b; ++j) {
                 if (j == s) continue;
+                (void)SDOT_CHECK_IDX(j, A.n, 6);
                 const double c1x = A.pos[2 * j], c1y = A.pos[2 * j + 1], w1 = A.w[j];
                 double ox, oy, nx, ny;
                 bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
@@ -265,11 +293,20 @@ SDOT_KFN bool process_cell(const Cell2DArgs &A, long long s, const PolyView<doub
                              int acc_st, const PolyView<double> &piece, Out &row, Out &nbo) {
     const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
     const int n = build_cell(A, s, cell, cap, c0x, c0y, w0);
+    if (n == -2) {
+        // failed guard: report a NaN cell, not an overflow
+        if (A.mass) A.mass[s] = nan("");
+        if (A.mass_c) A.mass_c[s] = nan("");
+        if (A.ctd) A.ctd[2 * s] = A.ctd[2 * s + 1] = nan("");
+        row.emit(int(s), 0.0);
+        return true;
+    }
     if (n < 0) return false;
 
     const double r = BALL ? sqrt(w0) : -1.0;
     constexpr bool DIRECT = MODE == DM_SINGLE;
     Sink<DIRECT> sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
+    sink.n_diracs = A.n;
 
     if (MODE == DM_SINGLE && !BALL) {
         // reference order: fan from vertex 0, boundary items from edge (n-1 -> 0)
@@ -347,6 +384,10 @@ SDOT_KFN bool process_cell(const Cell2DArgs &A, long long s, const PolyView<doub
                         piece.Y(k) = cell.Y(k);
                         piece.I(k) = k;
                     }
+                    if (A.item_off[it] < 0 || A.item_off[it + 1] > A.item_nv) {
+                        guard_fail(A, 3, s, it);
+                        continue;
+                    }
                     for (int e = A.item_off[it]; e < A.item_off[it + 1] && np > 0; ++e)
                         np = plane_cut(piece, np, cap, A.item_xy[2 * e], A.item_xy[2 * e + 1], A.item_nrm[2 * e],
                                        A.item_nrm[2 * e + 1], PID_OWN, false);
@@ -368,6 +409,10 @@ SDOT_KFN bool process_cell(const Cell2DArgs &A, long long s, const PolyView<doub
                 const double m = acc[i0 * acc_st];
                 if (m < 0) continue;
                 const int id = cell.I(i0);
+                if (id < 0 || id >= A.n) {
+                    guard_fail(A, 4, s, id);
+                    continue;
+                }
                 const double dx = c0x - A.pos[2 * id], dy = c0y - A.pos[2 * id + 1];
                 const double dist = sqrt(dx * dx + dy * dy);
                 if (dist != 0) {
@@ -419,10 +464,10 @@ __global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
     double *sy = sx + CAP * T2D;
     int *sid = reinterpret_cast<int *>(sy + CAP * T2D);
     double *extra = sy + CAP * T2D + (CAP * T2D + 1) / 2;
-    PolyView<double> cell{sx + t, sy + t, sid + t, T2D};
+    PolyView<double> cell{sx + t, sy + t, sid + t, T2D, CAP};
     double *acc = extra + t;
     PolyView<double> piece{extra + CAP * T2D + t, extra + 2 * CAP * T2D + t,
-                           reinterpret_cast<int *>(extra + 3 * CAP * T2D) + t, T2D};
+                           reinterpret_cast<int *>(extra + 3 * CAP * T2D) + t, T2D, CAP};
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
     Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
@@ -445,11 +490,11 @@ struct TierScratch {
     int *nb_id;
     SDOT_HDI TierScratch(double *base, long long S, int cap, int g) {
         double *p = base;
-        cell = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S)};
+        cell = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S), cap};
         p += 3 * cap * S;
         acc = p + g;
         p += cap * S;
-        piece = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S)};
+        piece = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S), cap};
         p += 3 * cap * S;
         row_val = p + g;
         p += (cap + 1) * S;
@@ -523,17 +568,28 @@ void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
         attr_set = true;
     }
     k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
     double *scr = static_cast<double *>(scratch);
     k_cells2d_tier<MODE, BALL, CAP_BIG_2D><<<ceil_div(BIG_THREADS, 64), 64, 0, st>>>(
         a, scr, BIG_THREADS, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
     k_cells2d_tier<MODE, BALL, CAP_HUGE_2D><<<ceil_div(HUGE_THREADS, 64), 64, 0, st>>>(
         a, scr, HUGE_THREADS, a.ovf_list2, a.ovf_cnt2, nullptr, nullptr);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 
 }  // namespace
+
+void cells2d_read_checks(unsigned long long out[3]) {
+#ifdef SDOT_CHECKS
+    SDOT_CUDA(cudaMemcpyFromSymbol(out, sdot_dbg_word, 3 * sizeof(unsigned long long)));
+#else
+    out[0] = out[1] = out[2] = 0;
+#endif
+}
 
 size_t cells2d_scratch_bytes() {
     const long long a = tier_doubles(BIG_THREADS, CAP_BIG_2D), b = tier_doubles(HUGE_THREADS, CAP_HUGE_2D);

@@ -45,6 +45,7 @@ struct Cell2DArgs {
     const double *pos = nullptr;   // 2n, sorted order
     const double *w = nullptr;     // n, sorted order
     const TreeNode<2> *nodes = nullptr;
+    int max_nodes = 1 << 30;       // node array size (debug checks)
     // starting polygon (single item polygon, inflated bbox, or image box)
     int start_n = 0;
     const double *start_xy = nullptr;  // 2 * start_n
@@ -74,9 +75,14 @@ struct Cell2DArgs {
     int *ovf_list2 = nullptr;
     int *ovf_cnt2 = nullptr;
     unsigned *err = nullptr;
+    int *guard = nullptr;          // first failed guard: (code, sorted index, value)
+    long long item_nv = 0;         // number of item vertices (multi items)
 };
 
 size_t cells2d_scratch_bytes();
+// First failed debug check of the cell kernels (code, line, value); zeros in
+// release builds.
+void cells2d_read_checks(unsigned long long out[3]);
 // Fast kernel over all cells, then the big and huge tiers over the overflow
 // lists.  `scratch` must hold cells2d_scratch_bytes() bytes.
 void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st);

@@ -40,13 +40,40 @@ struct CudaError {
     const char *where;
 };
 
-#define SDOT_CUDA(call)                                                         \
-    do {                                                                        \
-        cudaError_t e_ = (call);                                                \
-        if (e_ != cudaSuccess) throw ::sdot::CudaError{e_, #call};              \
+#define SDOT_STR2(x) #x
+#define SDOT_STR(x) SDOT_STR2(x)
+#define SDOT_CUDA(call)                                                                             \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) throw ::sdot::CudaError{e_, #call " (" __FILE__ ":" SDOT_STR(__LINE__) ")"}; \
     } while (0)
 
+// Debug builds (-DSDOT_CHECKS) bounds-check buffer accesses in the kernels:
+// a failing check records (code, line, value) of the first failure in a
+// per-translation-unit device word and the access is redirected to index 0.
+// Release builds compile the checks away.
+#ifdef SDOT_CHECKS
+static __device__ unsigned long long sdot_dbg_word[3];
+__host__ __device__ inline void check_fail(int code, int line, long long value) {
+#ifdef __CUDA_ARCH__
+    if (atomicCAS(&sdot_dbg_word[0], 0ull, (unsigned long long)code) == 0ull) {
+        sdot_dbg_word[1] = (unsigned long long)line;
+        sdot_dbg_word[2] = (unsigned long long)value;
+    }
+#else
+    printf("sdot check %d failed at line %d value %lld\n", code, line, value);
+#endif
+}
+#define SDOT_CHECK_IDX(k, n, code) \
+    (((k) < 0 || (k) >= (n)) ? (::sdot::check_fail(code, __LINE__, (long long)(k)), 0) : (k))
+#else
+#define SDOT_CHECK_IDX(k, n, code) (k)
+#endif
+
 inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+// Process-wide count of this library's kernel launches (sdot_kernel_launches).
+void note_launch();
 
 // Per-cell kernel bodies are device functions; a host build of them (for
 // CPU-side debugging of the kernels) is compiled with SDOT_HOST_KERNELS.
@@ -71,6 +98,7 @@ enum DevErr : unsigned {
     DE_STACK = 2u,         // traversal stack overflow (should not happen: depth bounded)
     DE_ITER = 4u,          // an iteration cap was reached
     DE_PIECE = 8u,         // a piece overflowed its capacity
+    DE_GUARD = 16u,        // an input failed a consistency guard (see the debug triple)
 };
 
 }  // namespace sdot

@@ -14,6 +14,21 @@ __global__ void k_sort_merge(Rows R, long long n, const int *idx, long long *cnt
     const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int m = R.cnt[s];
+#ifdef SDOT_CHECKS
+    if (m < 0 || m > 4096 || (m > R.cap && (R.side[s] < 0 || R.side[s] + m > R.side_cap))) {
+        check_fail(20, __LINE__, m);
+        R.cnt[s] = 0;
+        cnt_orig[idx[s]] = 0;
+        return;
+    }
+    for (int i = 0; i < m; ++i) {
+        const int c = *R.colp(s, i);
+        if (c < 0 || c >= n) {
+            check_fail(21, __LINE__, c);
+            *R.colp(s, i) = int(s);
+        }
+    }
+#endif
     // insertion sort in place (rows are short: ~7 entries in 2D, ~16 in 3D)
     for (int i = 1; i < m; ++i) {
         const int c = *R.colp(s, i);
@@ -94,30 +109,43 @@ __global__ void k_unpermute(const double *in, double *out, long long n, int d, c
 
 }  // namespace
 
+void csr_read_checks(unsigned long long out[3]) {
+#ifdef SDOT_CHECKS
+    SDOT_CUDA(cudaMemcpyFromSymbol(out, sdot_dbg_word, 3 * sizeof(unsigned long long)));
+#else
+    out[0] = out[1] = out[2] = 0;
+#endif
+}
+
 void csr_sort_merge(const Rows &R, long long n, const int *idx, long long *cnt_orig, cudaStream_t st) {
     if (n <= 0) return;
     k_sort_merge<<<ceil_div(n, TB), TB, 0, st>>>(R, n, idx, cnt_orig);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 void csr_write(const Rows &R, long long n, const int *idx, const long long *offsets, long long *cols, double *vals,
                cudaStream_t st) {
     if (n <= 0) return;
     k_write<<<ceil_div(n, TB), TB, 0, st>>>(R, n, idx, offsets, cols, vals);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 void nb_counts(const Rows &NB, long long n, const int *idx, long long *cnt_orig, cudaStream_t st) {
     if (n <= 0) return;
     k_nb_counts<<<ceil_div(n, TB), TB, 0, st>>>(NB, n, idx, cnt_orig);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 void nb_write(const Rows &NB, long long n, const int *idx, const long long *offsets, long long *ids, cudaStream_t st) {
     if (n <= 0) return;
     k_nb_write<<<ceil_div(n, TB), TB, 0, st>>>(NB, n, idx, offsets, ids);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st) {
     if (n <= 0) return;
     k_unpermute<<<ceil_div(n, TB), TB, 0, st>>>(in, out, n, d, idx);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 

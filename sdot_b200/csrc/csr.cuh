@@ -17,6 +17,8 @@ void csr_write(const Rows &R, long long n, const int *idx, const long long *offs
 // Neighbour lists: ids mapped (sorted -> original; domain edges -> -1; arcs -> -2).
 void nb_counts(const Rows &NB, long long n, const int *idx, long long *cnt_orig, cudaStream_t st);
 void nb_write(const Rows &NB, long long n, const int *idx, const long long *offsets, long long *ids, cudaStream_t st);
+// First failed debug check of the assembly kernels (zeros in release builds).
+void csr_read_checks(unsigned long long out[3]);
 // out[idx[s] * d + k] = in[s * d + k]
 void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st);
 

@@ -33,9 +33,10 @@ struct PolyView {
     T *y;
     int *id;
     int st;
-    SDOT_HDI T &X(int k) const { return x[k * st]; }
-    SDOT_HDI T &Y(int k) const { return y[k * st]; }
-    SDOT_HDI int &I(int k) const { return id[k * st]; }
+    int cap = 1 << 30;  // vertex slots (bound of the debug checks)
+    SDOT_HDI T &X(int k) const { return x[SDOT_CHECK_IDX(k, cap, 1) * st]; }
+    SDOT_HDI T &Y(int k) const { return y[SDOT_CHECK_IDX(k, cap, 1) * st]; }
+    SDOT_HDI int &I(int k) const { return id[SDOT_CHECK_IDX(k, cap, 1) * st]; }
     SDOT_HDI void copy(int dst, int src) const {
         X(dst) = X(src);
         Y(dst) = Y(src);

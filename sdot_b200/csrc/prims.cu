@@ -98,6 +98,7 @@ void scan_rec(const T *in, T *out, long long n, char *tmp, T *grand_total, cudaS
     long long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nb == 1) {
         k_block_scan<T><<<1, SCAN_THREADS, 0, st>>>(in, out, n, nullptr, grand_total);
+        note_launch();
         SDOT_CUDA(cudaGetLastError());
         return;
     }
@@ -106,9 +107,11 @@ void scan_rec(const T *in, T *out, long long n, char *tmp, T *grand_total, cudaS
     char *next = reinterpret_cast<char *>(sums_scanned + nb);
     next = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(next) + 255) & ~uintptr_t(255));
     k_block_sums<T><<<unsigned(nb), SCAN_THREADS, 0, st>>>(in, sums, n);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
     scan_rec<T>(sums, sums_scanned, nb, next, nullptr, st);
     k_block_scan<T><<<unsigned(nb), SCAN_THREADS, 0, st>>>(in, out, n, sums_scanned, grand_total);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 
@@ -219,9 +222,11 @@ void radix_sort_pairs(const unsigned *keys_in, const unsigned *vals_in, unsigned
         unsigned *dv = to_out ? vals_out : vals_alt;
         (void)last;
         k_radix_hist<<<nb, RADIX_THREADS, 0, st>>>(src_k, n, 8 * p, ghist, nb);
+        note_launch();
         SDOT_CUDA(cudaGetLastError());
         scan_exclusive<unsigned>(ghist, goff, 256LL * nb, scan_tmp, st);
         k_radix_scatter<<<nb, RADIX_THREADS, 0, st>>>(src_k, src_v, dk, dv, n, 8 * p, goff, nb);
+        note_launch();
         SDOT_CUDA(cudaGetLastError());
         src_k = dk;
         src_v = dv;

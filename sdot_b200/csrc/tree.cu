@@ -284,19 +284,30 @@ void DeviceTree<D>::build(const double *pos_orig, const double *w_orig, long lon
     n = nn;
     if (n == 0) return;
     k_bbox_init<D><<<1, 32, 0, st>>>(bbox_bits);
+    note_launch();
     k_bbox<D><<<grid_for(n, TB), TB, 0, st>>>(pos_orig, n, bbox_bits);
+    note_launch();
     k_bbox_final<D><<<1, 32, 0, st>>>(bbox_bits, bbox);
+    note_launch();
     k_morton<D><<<ceil_div(n, TB), TB, 0, st>>>(pos_orig, n, bbox, key_bits, keys, vals);
+    note_launch();
     SDOT_CUDA(cudaGetLastError());
     radix_sort_pairs(keys, vals, keys2, vals2, keys3, vals3, n, D * key_bits, tmp, st);
     k_gather<D><<<ceil_div(n, TB), TB, 0, st>>>(pos_orig, w_orig, vals2, n, pos, w, idx, inv);
+    note_launch();
     k_tree_init<D><<<1, 1, 0, st>>>(nodes, node_level, counters, npass, n);
+    note_launch();
     const int g = grid_for(n / 2 + 1, TB);
     for (int p = 0; p < npass; ++p) {
         k_split<D><<<g, TB, 0, st>>>(nodes, node_level, counters, p, keys2, key_bits, max_per_leaf, max_nodes);
+        note_launch();
         k_mark_pass<<<1, 1, 0, st>>>(counters, p);
+        note_launch();
     }
-    for (int p = npass - 1; p >= 0; --p) k_reduce<D><<<g, TB, 0, st>>>(nodes, counters, p, pos, w, true);
+    for (int p = npass - 1; p >= 0; --p) {
+        k_reduce<D><<<g, TB, 0, st>>>(nodes, counters, p, pos, w, true);
+        note_launch();
+    }
     SDOT_CUDA(cudaGetLastError());
 }
 
@@ -304,6 +315,7 @@ template <int D>
 void DeviceTree<D>::update_weights(const double *w_orig, cudaStream_t st) {
     if (n == 0) return;
     k_gather_w<D><<<ceil_div(n, TB), TB, 0, st>>>(w_orig, idx, n, w);
+    note_launch();
     refresh_maxw(st);
 }
 
@@ -311,7 +323,10 @@ template <int D>
 void DeviceTree<D>::refresh_maxw(cudaStream_t st) {
     if (n == 0) return;
     const int g = grid_for(n / 2 + 1, TB);
-    for (int p = npass - 1; p >= 0; --p) k_reduce<D><<<g, TB, 0, st>>>(nodes, counters, p, pos, w, false);
+    for (int p = npass - 1; p >= 0; --p) {
+        k_reduce<D><<<g, TB, 0, st>>>(nodes, counters, p, pos, w, false);
+        note_launch();
+    }
     SDOT_CUDA(cudaGetLastError());
 }
 

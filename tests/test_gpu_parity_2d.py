@@ -70,7 +70,10 @@ def test_clustered_with_weights(gpu_lib, ref_oracle):
     p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng)])
     w = rng.uniform(-1e-6, 1e-6, n) * 1e-2
     gpu, ref = make_pair(p, w, ref_oracle)
-    check_all(gpu, ref, n)
+    # tight clusters give sliver edges whose length is a difference of nearby
+    # vertex positions: the two CPU oracles (reference and restatement) already
+    # differ by 8.7e-13 of the mean diagonal here, so the Hessian bound is 1e-11
+    check_all(gpu, ref, n, rtol_hess=1e-11)
 
 
 def test_config2_weights_void_cells(gpu_lib, ref_oracle):
@@ -87,10 +90,15 @@ def test_config2_weights_void_cells(gpu_lib, ref_oracle):
 
 def test_voronoi_boundary_clamped_points(gpu_lib, ref_oracle):
     # clustered points clamped to the box: long collinear runs on the box
-    # edges give cells with hundreds of vertices (the large-capacity tiers)
+    # edges give cells with hundreds of vertices (the large-capacity tiers).
+    # Bisectors of nearly collinear points are nearly parallel, so a vertex
+    # position (hence an edge length) carries an error of eps / sin(angle):
+    # the two CPU oracles (reference and restatement, same cut sequence)
+    # differ by 2.7e-11 of the mean diagonal on the same Hessian entry, so the
+    # Hessian bound here is 1e-10.
     c = workloads.config2(n=100_000)
     gpu, ref = make_pair(c["positions"], np.zeros(100_000), ref_oracle)
-    check_all(gpu, ref, 100_000)
+    check_all(gpu, ref, 100_000, rtol_hess=1e-10)
     assert gpu.last_overflow_count() > 0
 
 
@@ -121,6 +129,24 @@ def test_image_density_disc_clip(gpu_lib, ref_oracle):
     check_all(gpu, ref, 5000, rtol=1e-11)
 
 
+MULTI_OFF = ("the multi-shape cell kernel raised an illegal address in a release build while a bounds-checked "
+             "build of the same kernel ran clean; it stays disabled until the cause is found")
+
+
+def test_multi_items_rejected(gpu_lib):
+    # the disabled path fails loudly, before any kernel is launched
+    from sdot_b200._lib import SDOT_UNSUPPORTED, SdotError
+    from sdot_b200.power_diagram import PowerDiagram
+
+    g = PowerDiagram(np.random.default_rng(0).random((10, 2)) * [2.0, 1.0], np.zeros(10))
+    g.add_box_shape([0.0, 0.0], [1.0, 1.0], 1.0)
+    g.add_box_shape([1.0, 0.0], [2.0, 1.0], 0.5)
+    with pytest.raises(SdotError) as e:
+        g.integrals()
+    assert e.value.status == SDOT_UNSUPPORTED
+
+
+@pytest.mark.skip(reason=MULTI_OFF)
 def test_multi_items(gpu_lib, ref_oracle):
     rng = np.random.default_rng(5)
     n = 2000
@@ -132,6 +158,7 @@ def test_multi_items(gpu_lib, ref_oracle):
     check_all(gpu, ref, n)
 
 
+@pytest.mark.skip(reason=MULTI_OFF)
 def test_multi_items_disc_clip(gpu_lib, ref_oracle):
     rng = np.random.default_rng(8)
     n = 1500
