@@ -113,6 +113,50 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
  * domain edge, -2 for a disc arc.  Two-phase like the Hessian.               */
 int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *count_inout, int mem_space);
 
+/* ---- Newton on the weights -------------------------------------------------
+ * Replaces OptimalTransportSolver::solve( positions, weights, n, masses, rf )
+ * (OptimalTransportSolver.tcc:27-119) and its sparse direct solve
+ * EigenSolver::solve (EigenSolver.cpp:9-41).  Each iteration evaluates the
+ * masses and the CSR Hessian on the device, applies the reference's gauge fix
+ * (the Hessian entry (0,0) doubled when there is no ball cut, .tcc:62-63),
+ * solves H dw = m - target by Jacobi-preconditioned conjugate gradients on
+ * the device and sets w -= tau dw.
+ *   damping = 0: the reference rule: tau = 1; when a cell is empty the step
+ *                is undone as w = 0.9 w_old + 0.1 w (.tcc:72-79).
+ *   damping = 1: Kitagawa-Merigot-Thibert damping: tau halves until every
+ *                cell keeps at least half of min(min target, min starting
+ *                mass) and |m - target| drops by the factor (1 - tau / 2).
+ * Stops when max_i |m_i - target_i| / target_i <= rel_mass_tol (the
+ * reference stops on max |dw| < 1e-6, .tcc:111-112).  The solved weights
+ * stay in the context (sdot_get_weights).                                    */
+typedef struct sdot_newton_opts {
+    int max_iter;          /* Newton iterations (reference: max_nb_iter = 150, .tcc:16) */
+    double rel_mass_tol;   /* stopping tolerance on the relative mass error */
+    int pcg_max_iter;      /* conjugate-gradient iterations per Newton step */
+    double pcg_rel_tol;    /* |H dw - b| <= pcg_rel_tol |b| */
+    int damping;           /* 0: reference rule, 1: KMT step halving */
+    int verbosity;         /* > 0: one line per Newton iteration on stderr */
+} sdot_newton_opts;
+
+typedef struct sdot_newton_report {
+    int iterations;            /* Newton iterations done */
+    int64_t pcg_iterations;    /* conjugate-gradient iterations, all steps */
+    double max_rel_mass_error; /* at the returned weights */
+    double min_mass;           /* smallest cell mass at the returned weights */
+    double time_ms;            /* wall time of the solve */
+    int evaluations;           /* fused cell evaluations done */
+} sdot_newton_report;
+
+/* target: double[n] masses (mem_space says where).  opts may be NULL for the
+ * defaults {150, 1e-10, 20000, 1e-12, 1, 0}; report may be NULL.
+ * Returns SDOT_OK, SDOT_NOT_CONVERGED (iteration or step-halving cap),
+ * SDOT_VOID_CELL (damping = 1 and a cell is empty at the start weights) or
+ * an evaluation error.                                                        */
+int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_newton_opts *opts,
+               sdot_newton_report *report);
+/* Current weights, double[n] in the caller's Dirac order. */
+int sdot_get_weights(sdot_ctx *ctx, double *out, int mem_space);
+
 /* Fused evaluation only, results kept on the device (for timing). */
 int sdot_evaluate(sdot_ctx *ctx);
 /* Device time in milliseconds of the last evaluation stages:

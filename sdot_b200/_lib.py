@@ -78,6 +78,9 @@ SIGNATURES = {
     "sdot_get_centroids": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "sdot_get_der_integrals_wrt_weights": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int]),
     "sdot_get_neighbors": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int]),
+    "sdot_solve": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.POINTER(SdotNewtonOptions),
+                                  ctypes.POINTER(SdotNewtonReport)]),
+    "sdot_get_weights": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "sdot_evaluate": (ctypes.c_int, [_P]),
     "sdot_last_timings": (ctypes.c_int, [_P, _P]),
     "sdot_last_overflow_count": (ctypes.c_int, [_P, _P]),

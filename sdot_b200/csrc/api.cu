@@ -4,10 +4,13 @@
 #include "csr.cuh"
 #include "geom2d.cuh"
 #include "prims.cuh"
+#include "solve.cuh"
 #include "tree.cuh"
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cmath>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -135,6 +138,7 @@ struct sdot_ctx {
         dfree(d_pos); dfree(d_w);
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
         free_eval();
+        free_newton();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -371,6 +375,136 @@ struct sdot_ctx {
     }
 
     void mark_dirty() { eval_dirty = nb_dirty = true; }
+
+    // ---- Newton on the weights (OptimalTransportSolver::solve, .tcc:27-119)
+    long long ncap = 0;
+    double *t_orig = nullptr, *t_sorted = nullptr, *w_old = nullptr, *dir = nullptr, *rhs = nullptr;
+    double *pcg_buf = nullptr, *red = nullptr;
+    PcgWork pcg;
+
+    void free_newton() {
+        dfree(t_orig); dfree(t_sorted); dfree(w_old); dfree(dir); dfree(rhs); dfree(pcg_buf); dfree(red);
+        ncap = 0;
+    }
+    void reserve_newton() {
+        if (ncap >= n && t_orig) return;
+        free_newton();
+        ncap = std::max<long long>(n, 1);
+        dalloc(t_orig, ncap); dalloc(t_sorted, ncap); dalloc(w_old, ncap); dalloc(dir, ncap); dalloc(rhs, ncap);
+        dalloc(pcg_buf, pcg_work_doubles(ncap));
+        dalloc(red, 3 * PCG_BLOCKS + 8);
+        pcg_bind(pcg, pcg_buf, ncap);
+    }
+    // e[0] = max_i |m_i - t_i| / t_i, e[1] = min_i m_i, e[2] = sum_i (m_i - t_i)^2 (sorted order)
+    void mass_stats(const double *m, double e[3]) {
+        mass_errors(m, t_sorted, n, red, red + 3 * PCG_BLOCKS, stream);
+        SDOT_CUDA(cudaMemcpyAsync(e, red + 3 * PCG_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaStreamSynchronize(stream));
+    }
+    void set_device_weights_changed() {
+        w_dirty = true;
+        mark_dirty();
+    }
+
+    int solve(const double *target, int mem_space, const sdot_newton_opts &o, sdot_newton_report &rep) {
+        const auto t_start = std::chrono::steady_clock::now();
+        rep = sdot_newton_report{};
+        if (n == 0) throw BadArg("no Diracs: call sdot_set_diracs first");
+        if (!target) throw BadArg("null target masses");
+        if (o.max_iter < 0 || o.pcg_max_iter <= 0 || !(o.rel_mass_tol >= 0) || !(o.pcg_rel_tol > 0))
+            throw BadArg("bad Newton options");
+        reserve_newton();
+        upload_target(target, mem_space);
+        int st = evaluate();
+        ++rep.evaluations;
+        if (st != SDOT_OK) return st;
+        // targets in sorted (tree) order; the order is fixed while the positions are
+        gather_sorted(t_orig, tree2.idx, t_sorted, n, stream);
+        double et[3];
+        mass_stats(t_sorted, et);  // et[1] = min target
+        if (!(et[1] > 0)) throw BadArg("target masses must be positive");
+        // gauge fix on the row of Dirac 0 (.tcc:62-63), only without ball cut
+        long long gauge = -1;
+        if (!ball) {
+            int g = 0;
+            SDOT_CUDA(cudaMemcpyAsync(&g, tree2.inv, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            SDOT_CUDA(cudaStreamSynchronize(stream));
+            gauge = g;
+        }
+        SDOT_CUDA(cudaMemcpyAsync(w_old, d_w, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        double e[3];
+        mass_stats(s_mass, e);
+        if (o.damping && !(e[1] > 0)) {
+            last_error = "a cell is empty at the start weights (damped Newton keeps every cell non-empty)";
+            return SDOT_VOID_CELL;
+        }
+        const double eps0 = 0.5 * std::min(et[1], e[1]);
+        int status = SDOT_NOT_CONVERGED;
+        for (int it = 0;; ++it) {
+            rep.max_rel_mass_error = e[0];
+            rep.min_mass = e[1];
+            if (o.verbosity > 0)
+                fprintf(stderr, "sdot newton %d: max rel mass error %.3e, min mass %.3e\n", it, e[0], e[1]);
+            if (e[0] <= o.rel_mass_tol) {
+                status = SDOT_OK;
+                break;
+            }
+            if (it >= o.max_iter) break;
+            rep.iterations = it + 1;
+            if (!o.damping && !(e[1] > 0)) {
+                // reference back-off on an empty cell: w = 0.9 w_old + 0.1 w (.tcc:72-79)
+                axpby(w_old, d_w, d_w, 0.9, 0.1, n, stream);
+                set_device_weights_changed();
+                st = evaluate();
+                ++rep.evaluations;
+                if (st != SDOT_OK) return st;
+                mass_stats(s_mass, e);
+                continue;
+            }
+            SDOT_CUDA(cudaMemcpyAsync(w_old, d_w, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            axpby(s_mass, t_sorted, rhs, 1.0, -1.0, n, stream);  // v_values -= masses (.tcc:89-90)
+            const PcgResult pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream);
+            rep.pcg_iterations += pr.iterations;
+            if (o.verbosity > 0)
+                fprintf(stderr, "sdot newton %d: pcg %d iterations, relative residual %.3e\n", it, pr.iterations,
+                        pr.rel_residual);
+            double tau = 1.0, en[3];
+            bool accepted = false;
+            for (int k = 0; k <= 40; ++k) {
+                apply_step(w_old, dir, tree2.idx, tau, d_w, n, stream);  // weights -= dw (.tcc:106-109)
+                set_device_weights_changed();
+                st = evaluate();
+                ++rep.evaluations;
+                if (st != SDOT_OK) return st;
+                mass_stats(s_mass, en);
+                if (!o.damping || en[0] <= o.rel_mass_tol ||
+                    (en[1] >= eps0 && std::sqrt(en[2]) <= (1.0 - 0.5 * tau) * std::sqrt(e[2]))) {
+                    accepted = true;
+                    break;
+                }
+                tau *= 0.5;
+            }
+            if (!accepted) {
+                // no acceptable step: keep the last accepted weights
+                SDOT_CUDA(cudaMemcpyAsync(d_w, w_old, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+                set_device_weights_changed();
+                last_error = "damped Newton: no step length decreased the mass error";
+                break;
+            }
+            e[0] = en[0];
+            e[1] = en[1];
+            e[2] = en[2];
+        }
+        rep.time_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        if (status == SDOT_NOT_CONVERGED && last_error.empty()) last_error = "Newton did not reach the tolerance";
+        return status;
+    }
+
+    void upload_target(const double *target, int mem_space) {
+        SDOT_CUDA(cudaMemcpyAsync(t_orig, target, size_t(n) * sizeof(double),
+                                  mem_space == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream));
+    }
 };
 
 namespace {
@@ -760,6 +894,28 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
         dfree(tmp);
         *count_inout = tot;
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_newton_opts *opts,
+               sdot_newton_report *report) {
+    return guarded(ctx, [&] {
+        sdot_newton_opts o{150, 1e-10, 20000, 1e-12, 1, 0};
+        if (opts) o = *opts;
+        sdot_newton_report r{};
+        ctx->last_error.clear();
+        const int st = ctx->solve(target, mem_space, o, r);
+        if (report) *report = r;
+        return st;
+    });
+}
+
+int sdot_get_weights(sdot_ctx *ctx, double *out, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!out) throw BadArg("null output");
+        if (ctx->n) ctx->copy_out(out, ctx->d_w, size_t(ctx->n) * sizeof(double), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
         return int(SDOT_OK);
     });
 }

@@ -1,0 +1,50 @@
+// Device linear algebra for Newton on the weights: Jacobi-preconditioned
+// conjugate gradient on the Hessian rows (ELL + side buffer, sorted order).
+//
+// Replaces the reference's sparse direct solve EigenSolver::solve
+// (src/sdot/Solvers/EigenSolver.cpp:9-41, Eigen::SimplicialCholesky) used by
+// OptimalTransportSolver::solve (src/sdot/Solvers/OptimalTransportSolver.tcc:97-101).
+#pragma once
+#include "cell2d.cuh"
+#include "common.cuh"
+
+namespace sdot {
+
+// Scratch of one PCG solve over n rows (device buffers owned by the caller).
+struct PcgWork {
+    double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
+    double *partial = nullptr;  // PCG_BLOCKS partial sums (x 2)
+    double *scal = nullptr;     // device scalars (see solve.cu)
+};
+constexpr int PCG_BLOCKS = 148 * 4;
+
+size_t pcg_work_doubles(long long n);
+void pcg_bind(PcgWork &w, double *base, long long n);
+
+struct PcgResult {
+    int iterations = 0;
+    double rel_residual = 0;
+    bool converged = false;
+};
+
+// Solves (H + g e_g e_g^T) x = b where H is given by `rows` (sorted order,
+// n rows) and the optional gauge term doubles the diagonal of row `gauge_row`
+// (the reference's m_values[0] *= 2, OptimalTransportSolver.tcc:62-63);
+// gauge_row < 0 disables it.  x starts at 0.  Stops when
+// |r| <= rel_tol |b| or after max_iter iterations (checked every `check`
+// iterations, the only host synchronisations).
+PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
+                    int max_iter, const PcgWork &w, cudaStream_t st, int check = 32);
+
+// Device reductions used by the Newton loop (deterministic order).
+// out[0] = max_i |m_i - t_i| / t_i, out[1] = min_i m_i, out[2] = sum_i (m_i - t_i)^2
+void mass_errors(const double *m, const double *t, long long n, double *partial, double *out, cudaStream_t st);
+// r = m - t
+void axpby(const double *a, const double *b, double *out, double alpha, double beta, long long n, cudaStream_t st);
+// w_orig[idx[s]] = w_base_orig[idx[s]] - tau * d_sorted[s]
+void apply_step(const double *w_base, const double *d_sorted, const int *idx, double tau, double *w_out, long long n,
+                cudaStream_t st);
+// t_sorted[s] = t_orig[idx[s]]
+void gather_sorted(const double *t_orig, const int *idx, double *t_sorted, long long n, cudaStream_t st);
+
+}  // namespace sdot

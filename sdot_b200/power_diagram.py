@@ -175,6 +175,25 @@ class PowerDiagram:
                                                  SDOT_HOST))
         return offsets, ids
 
+    def solve_weights(self, target_masses, rel_mass_tol=1e-10, max_iter=150, damping=True, pcg_rel_tol=1e-12,
+                      pcg_max_iter=20000, verbosity=0):
+        """Newton on the weights so that every cell mass reaches its target
+        (OptimalTransportSolver::solve, OptimalTransportSolver.tcc:27-119).
+        Updates the weights of this diagram and returns the solver report as
+        a dict; raises SdotError when the tolerance is not reached."""
+        t = _f64(target_masses, (self.nb_diracs,))
+        opt = _lib.SdotNewtonOptions(int(max_iter), float(rel_mass_tol), int(pcg_max_iter), float(pcg_rel_tol),
+                                     int(bool(damping)), int(verbosity))
+        rep = _lib.SdotNewtonReport()
+        st = self._lib.sdot_solve(self._ctx, _ptr(t), SDOT_HOST, ctypes.byref(opt), ctypes.byref(rep))
+        w = np.empty(self.nb_diracs)
+        self._check(self._lib.sdot_get_weights(self._ctx, _ptr(w), SDOT_HOST))
+        self._weights = w
+        report = {f: getattr(rep, f) for f, _ in rep._fields_}
+        report["status"] = st
+        self._check(st)
+        return report
+
     def evaluate(self):
         """Fused evaluation kept on the device (timing helper)."""
         self._check(self._lib.sdot_evaluate(self._ctx))

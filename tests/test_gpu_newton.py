@@ -1,0 +1,109 @@
+"""Newton on the weights on the GPU vs the Newton oracle (compiled reference
+CSR + a direct sparse solve, oracle/newton.py).
+
+Both solves run to a relative mass error of 1e-12 from the same start; the
+gauge fix pins the weight of Dirac 0, so the weights themselves are compared:
+|w_gpu - w_ref| <= 1e-10 max |w_ref| (the round-off of a 1e-12 mass error
+amplified by the inverse Hessian, whose norm grows like n).
+"""
+import numpy as np
+import pytest
+
+from oracle import newton
+from sdot_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+W_RTOL = 1e-10
+
+
+def solve_pair(ref_oracle, p, w0, target, radial_func="unit", image=None, rule="damped", tol=1e-12):
+    from sdot_b200.power_diagram import PowerDiagram
+
+    gpu = PowerDiagram(p, w0, radial_func=radial_func)
+    ref = ref_oracle.RefPowerDiagram(p, w0, radial_func=radial_func)
+    if image is not None:
+        gpu.set_image_density(image)
+        ref.set_image_density(image)
+    else:
+        gpu.add_box_shape([0.0, 0.0], [1.0, 1.0])
+        ref.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    rep = gpu.solve_weights(target, rel_mass_tol=tol, damping=(rule == "damped"))
+    w_r, rep_r = newton.solve(ref, target, w0, tol=tol, rule=rule, ball_cut=(radial_func != "unit"))
+    assert rep_r["converged"]
+    return gpu, gpu.get_weights(), w_r, rep, rep_r
+
+
+def check_weights(w_g, w_r):
+    err = np.abs(w_g - w_r).max() / np.abs(w_r).max()
+    assert err <= W_RTOL, f"weights differ by {err:.3e} of max |w|"
+
+
+@pytest.mark.parametrize("rule", ["damped", "reference"])
+def test_newton_config1(gpu_lib, ref_oracle, rule):
+    c = workloads.config1()
+    n = len(c["weights"])
+    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, c["positions"], c["weights"], np.full(n, 1.0 / n), rule=rule)
+    assert rep["max_rel_mass_error"] <= 1e-12
+    check_weights(w_g, w_r)
+    m = gpu.integrals()
+    assert np.abs(m * n - 1).max() <= 1e-12
+
+
+def test_newton_clustered(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(11)
+    n = 5000
+    p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng)])
+    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, p, np.zeros(n), np.full(n, 1.0 / n))
+    check_weights(w_g, w_r)
+
+
+def test_newton_disc_clip_partial(gpu_lib, ref_oracle):
+    # partial transport: cells clipped by the disc of radius sqrt(w_i), total
+    # target 0.8 of the unit box; no gauge fix (the arcs make H regular)
+    rng = np.random.default_rng(12)
+    n = 2000
+    p = rng.random((n, 2))
+    w0 = np.full(n, (0.5 / np.sqrt(n)) ** 2)
+    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, p, w0, np.full(n, 0.8 / n), radial_func="in_ball_w05")
+    check_weights(w_g, w_r)
+
+
+def test_newton_image_density(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(13)
+    n = 3000
+    p = rng.random((n, 2))
+    img = workloads.c3_image(res=64)
+    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, p, np.zeros(n), np.full(n, 0.8 / n), image=img)
+    check_weights(w_g, w_r)
+
+
+def test_optimal_transport_facade_collinear_pairs(gpu_lib, ref_oracle):
+    # the reference's example: 20 pairs of close Diracs on the line y = 0.5
+    # (every cell a vertical strip), default unit box and equal masses
+    from sdot_b200.optimal_transport import OptimalTransport
+
+    xs = np.linspace(0, 1 - 1e-3, 20)
+    pos = np.array([[x + d, 0.5] for x in xs for d in (0.0, 1e-3)])
+    ot = OptimalTransport(pos)
+    ot.adjust_weights()
+    w_g = ot.get_weights()
+    m = ot.get_integrals()
+    assert np.abs(m * 40 - 1).max() <= 1e-10
+    ref = ref_oracle.RefPowerDiagram(pos, np.zeros(40))
+    ref.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    w_r, _ = newton.solve(ref, np.full(40, 1 / 40), np.zeros(40), tol=1e-10)
+    assert np.abs(w_g - w_r).max() <= 1e-9 * np.abs(w_r).max()
+
+
+def test_void_start_rejected_by_damped_newton(gpu_lib):
+    from sdot_b200._lib import SDOT_VOID_CELL, SdotError
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config2(n=20_000)
+    g = PowerDiagram(c["positions"], c["weights"])
+    g.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    assert (g.integrals() == 0).any()
+    with pytest.raises(SdotError) as e:
+        g.solve_weights(np.full(20_000, 1 / 20_000))
+    assert e.value.status == SDOT_VOID_CELL
