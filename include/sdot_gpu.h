@@ -157,6 +157,23 @@ int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_ne
 /* Current weights, double[n] in the caller's Dirac order. */
 int sdot_get_weights(sdot_ctx *ctx, double *out, int mem_space);
 
+/* EigenSolver::solve( x, offsets, columns, values, b ) (EigenSolver.cpp:9-41):
+ * solves H x = b for the n x n CSR matrix H (offsets[n + 1], columns[nnz],
+ * values[nnz], symmetric positive definite; the output of
+ * sdot_get_der_integrals_wrt_weights after the gauge fix).  gauge_fix != 0
+ * doubles the diagonal entry of row 0 first, as the reference does before
+ * its solve (m_values[0] *= 2, OptimalTransportSolver.tcc:62-63).  Jacobi-
+ * preconditioned conjugate gradients on the device from x = 0, stopping at
+ * |H x - b| <= rel_tol |b| or after max_iter iterations (the reference uses a
+ * sparse Cholesky factorisation).  All buffers in mem_space; work buffers
+ * are allocated for the call.  iterations / rel_residual may be NULL;
+ * errbuf (may be NULL) receives the message of a failure.
+ * Returns SDOT_OK, SDOT_NOT_CONVERGED, SDOT_BAD_ARG, SDOT_OOM or SDOT_CUDA_ERROR. */
+int sdot_csr_solve(const int64_t *offsets, const int64_t *columns, const double *values, int64_t n,
+                   const double *b, double *x, int gauge_fix, double rel_tol, int max_iter, int mem_space,
+                   int64_t *iterations, double *rel_residual, char *errbuf, int64_t errbuf_len);
+
+
 /* Fused evaluation only, results kept on the device (for timing). */
 int sdot_evaluate(sdot_ctx *ctx);
 /* Device time in milliseconds of the last evaluation stages:

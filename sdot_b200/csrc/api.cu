@@ -119,7 +119,7 @@ struct sdot_ctx {
     double *o_mass = nullptr, *o_mass_c = nullptr, *o_ctd = nullptr;
     Rows rows, nb;             // Hessian rows, boundary id lists (sorted order)
     long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
-    int *ovf_list = nullptr, *ovf_cnt = nullptr, *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;
+    int *ovf_list = nullptr, *ovf_cnt = nullptr;
     unsigned *err = nullptr;
     int *guard = nullptr;
     long long item_nv = 0;
@@ -148,7 +148,7 @@ struct sdot_ctx {
         free_rows(rows);
         free_rows(nb);
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
-        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err); dfree(guard);
+        dfree(ovf_list); dfree(ovf_cnt); dfree(err); dfree(guard);
         if (scratch) cudaFree(scratch);
         if (scan_tmp) cudaFree(scan_tmp);
         scratch = scan_tmp = nullptr;
@@ -188,8 +188,6 @@ struct sdot_ctx {
         dalloc(offsets, ecap + 1);
         dalloc(ovf_list, ecap);
         dalloc(ovf_cnt, 1);
-        dalloc(ovf_list2, ecap);
-        dalloc(ovf_cnt2, 1);
         dalloc(err, 1);
         dalloc(guard, 3);
         SDOT_CUDA(cudaMalloc(&scratch, cells2d_scratch_bytes()));
@@ -279,8 +277,6 @@ struct sdot_ctx {
         a.item_coeff = d_item_coeff;
         a.ovf_list = ovf_list;
         a.ovf_cnt = ovf_cnt;
-        a.ovf_list2 = ovf_list2;
-        a.ovf_cnt2 = ovf_cnt2;
         a.err = err;
         return a;
     }
@@ -337,6 +333,10 @@ struct sdot_ctx {
     }
 
     int finish_status() {
+        if (last_err & DE_ITER) {
+            last_error = "a tree traversal visited more nodes than the tree holds (inconsistent tree)";
+            return SDOT_ITER_CAP;
+        }
         if (last_err & DE_CAPACITY) {
             last_error = "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
             return SDOT_CAPACITY;
@@ -488,7 +488,10 @@ struct sdot_ctx {
                 // no acceptable step: keep the last accepted weights
                 SDOT_CUDA(cudaMemcpyAsync(d_w, w_old, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
                 set_device_weights_changed();
-                last_error = "damped Newton: no step length decreased the mass error";
+                char buf[160];
+                snprintf(buf, sizeof buf,
+                         "damped Newton: no step length decreased the mass error (max relative mass error %.3e)", e[0]);
+                last_error = buf;
                 break;
             }
             e[0] = en[0];
@@ -909,6 +912,73 @@ int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_ne
         if (report) *report = r;
         return st;
     });
+}
+
+int sdot_csr_solve(const int64_t *offsets, const int64_t *columns, const double *values, int64_t n, const double *b,
+                   double *x, int gauge_fix, double rel_tol, int max_iter, int mem_space, int64_t *iterations,
+                   double *rel_residual, char *errbuf, int64_t errbuf_len) {
+    auto err = [&](int code, const std::string &msg) {
+        if (errbuf && errbuf_len > 0) {
+            const size_t k = std::min<size_t>(msg.size(), size_t(errbuf_len - 1));
+            std::memcpy(errbuf, msg.data(), k);
+            errbuf[k] = 0;
+        }
+        return code;
+    };
+    if (n < 0 || (n > 0 && (!offsets || !columns || !values || !b || !x)) || max_iter <= 0 || !(rel_tol > 0))
+        return err(SDOT_BAD_ARG, "bad CSR solve arguments");
+    if (errbuf && errbuf_len > 0) errbuf[0] = 0;
+    if (n == 0) return SDOT_OK;
+    cudaStream_t st = nullptr;
+    long long *d_off = nullptr, *d_col = nullptr;
+    double *d_val = nullptr, *d_b = nullptr, *d_x = nullptr, *work = nullptr;
+    auto release = [&] {
+        if (mem_space != SDOT_DEVICE) {
+            dfree(d_off); dfree(d_col); dfree(d_val); dfree(d_b); dfree(d_x);
+        }
+        dfree(work);
+        if (st) cudaStreamDestroy(st);
+    };
+    try {
+        SDOT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        long long nnz = 0;
+        if (mem_space == SDOT_DEVICE) {
+            SDOT_CUDA(cudaMemcpyAsync(&nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
+            SDOT_CUDA(cudaStreamSynchronize(st));
+            d_off = (long long *)offsets;
+            d_col = (long long *)columns;
+            d_val = (double *)values;
+            d_b = (double *)b;
+            d_x = x;
+        } else {
+            nnz = offsets[n];
+            dalloc(d_off, size_t(n) + 1);
+            dalloc(d_col, size_t(nnz));
+            dalloc(d_val, size_t(nnz));
+            dalloc(d_b, size_t(n));
+            dalloc(d_x, size_t(n));
+            SDOT_CUDA(cudaMemcpyAsync(d_off, offsets, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+            SDOT_CUDA(cudaMemcpyAsync(d_col, columns, nnz * sizeof(long long), cudaMemcpyHostToDevice, st));
+            SDOT_CUDA(cudaMemcpyAsync(d_val, values, nnz * sizeof(double), cudaMemcpyHostToDevice, st));
+            SDOT_CUDA(cudaMemcpyAsync(d_b, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        dalloc(work, pcg_work_doubles(n));
+        PcgWork w;
+        pcg_bind(w, work, n);
+        const PcgResult r = pcg_solve_csr(CsrMat{d_off, d_col, d_val}, n, gauge_fix ? 0 : -1, d_b, d_x, rel_tol,
+                                          max_iter, w, st);
+        if (mem_space != SDOT_DEVICE)
+            SDOT_CUDA(cudaMemcpyAsync(x, d_x, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SDOT_CUDA(cudaStreamSynchronize(st));
+        if (iterations) *iterations = r.iterations;
+        if (rel_residual) *rel_residual = r.rel_residual;
+        release();
+        return r.converged ? int(SDOT_OK) : err(SDOT_NOT_CONVERGED, "conjugate gradients did not reach the tolerance");
+    } catch (const CudaError &e) {
+        release();
+        return err(e.err == cudaErrorMemoryAllocation ? SDOT_OOM : SDOT_CUDA_ERROR,
+                   std::string(cudaGetErrorString(e.err)) + " in " + e.where);
+    }
 }
 
 int sdot_get_weights(sdot_ctx *ctx, double *out, int mem_space) {

@@ -35,8 +35,7 @@ namespace {
 
 constexpr int T2D = 64;     // threads per block of the fast kernel
 constexpr int STACK = 64;   // traversal stack (depth <= 17 levels, <= 3 pending siblings each)
-constexpr int BIG_THREADS = 148 * 64;
-constexpr int HUGE_THREADS = 148 * 4;
+constexpr int WTIER_WARPS = 148 * 4;  // warps of the warp-per-cell tier (4 per SM)
 
 // Records the first failed consistency guard and flags the error word; the
 // caller then skips the access.  Guards cover every index that comes from
@@ -203,10 +202,23 @@ SDOT_HDI void stream_piece(const PolyView<double> &piece, int n, Stage &st) {
     st.finish();
 }
 
-// Builds the Laguerre cell of sorted Dirac s (before any disc clipping).
-// Returns the vertex count, or -1 on capacity overflow.
+// Builds the Laguerre cell of sorted Dirac s (before any disc clipping) as a
+// machine of uniform steps, so that the 32 cells of a warp advance together.
+// The walk is SpZGrid::for_each_laguerre_cell's (SpZGrid.tcc:494-719): boxes
+// popped nearest-first (children pushed farthest-first, keyed on the float
+// squared distance from c0 to the box centre as the reference's queue),
+// skipped when the eviction test holds for every vertex (SpZGrid.tcc:475-480),
+// a leaf's Diracs cut in index order (bisector SpZGrid.tcc:506-522).
+// Every step -- a node test or one cut -- is the same pass over the vertices:
+// a cut classifies each vertex by its side of the bisector, a node test asks
+// whether some vertex fails the eviction test; both quantities are computed
+// for every vertex and the step's one is kept, so lanes on different kinds of
+// steps run the same instructions.  Only the application of an effective cut
+// and the handling of a needed node branch.
+// Returns the vertex count, -1 on capacity (or stack / visit cap) overflow,
+// -2 on a failed guard.
 SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double c0x, double c0y,
-                          double w0) {
+                        double w0) {
     int n = A.start_n;
     for (int k = 0; k < n; ++k) {
         cell.X(k) = A.start_xy[2 * k];
@@ -216,29 +228,65 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
     int stack[STACK];
     int sp = 0;
     stack[sp++] = 0;
-    while (sp > 0) {
-        const int node = stack[--sp];
-        const TreeNode<2> nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
-        // SpZGrid::can_be_evicted: skip the box when no Dirac in it can be
-        // closer (in power distance) than c0 to any current vertex.
-        bool evict = true;
+    int j = 0, je = 0;  // Diracs of the current leaf still to cut by
+    int visits = 0;
+    while (true) {
+        // ---- the step: one cut (j < je) or one node test
+        const bool is_cut = j < je;
+        double ox = 0, oy = 0, nx = 0, ny = 0;
+        double lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0, maxw = 0;
+        int node = -1, nd_a = 0, nd_b = 0;
+        if (is_cut) {
+            if (j == s) {
+                ++j;
+                continue;
+            }
+            (void)SDOT_CHECK_IDX(j, A.n, 6);
+            bisector(c0x, c0y, w0, A.pos[2 * j], A.pos[2 * j + 1], A.w[j], ox, oy, nx, ny);
+        } else {
+            if (sp == 0) break;
+            if (++visits > A.max_nodes) {  // a tree visits each node once: a cycle means a corrupt tree
+                flag_error(A.err, DE_ITER);
+                return -1;
+            }
+            node = stack[--sp];
+            const TreeNode<2> &nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
+            lo0 = nd.lo[0];
+            lo1 = nd.lo[1];
+            hi0 = nd.hi[0];
+            hi1 = nd.hi[1];
+            maxw = nd.maxw;
+            nd_a = nd.a;
+            nd_b = nd.b;
+        }
+        // ---- the vertex pass shared by both kinds of step
+        CutFacts f;
         for (int k = 0; k < n; ++k) {
             const double px = cell.X(k), py = cell.Y(k);
-            const double qx = fmin(nd.hi[0], fmax(nd.lo[0], px));
-            const double qy = fmin(nd.hi[1], fmax(nd.lo[1], py));
+            const double d = (ox - px) * nx + (oy - py) * ny;
+            const double qx = fmin(hi0, fmax(lo0, px)), qy = fmin(hi1, fmax(lo1, py));
             const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
-            const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - nd.maxw;
-            if (!(lhs <= rhs)) {
-                evict = false;
-                break;
-            }
+            const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - maxw;
+            f.add(k, n, is_cut ? d < 0.0 : !(lhs <= rhs));
         }
-        if (evict) continue;
-        if (nd.b < 0) {
-            const int first = nd.a, nch = -nd.b;
+        if (is_cut) {
+            if (f.nb_out) {
+                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
+                if (n <= 0) return n;
+            }
+            ++j;
+            continue;
+        }
+        if (f.nb_out == 0) continue;  // every vertex passes: the box is evicted
+        if (nd_b < 0) {
+            const int first = nd_a, nch = -nd_b;
             if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
                 guard_fail(A, 1, s, node);
                 return -2;
+            }
+            if (sp + nch > STACK) {
+                flag_error(A.err, DE_STACK);
+                return -1;
             }
             float key[4];
             int ch[4];
@@ -249,50 +297,39 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 key[c] = float(mx * mx + my * my);
                 ch[c] = first + c;
             }
-            // insertion sort, farthest first
-            for (int i = 1; i < nch; ++i) {
+            for (int i = 1; i < nch; ++i) {  // farthest first
                 const float kk = key[i];
                 const int cc = ch[i];
-                int j = i - 1;
-                while (j >= 0 && key[j] < kk) {
-                    key[j + 1] = key[j];
-                    ch[j + 1] = ch[j];
-                    --j;
+                int q = i - 1;
+                while (q >= 0 && key[q] < kk) {
+                    key[q + 1] = key[q];
+                    ch[q + 1] = ch[q];
+                    --q;
                 }
-                key[j + 1] = kk;
-                ch[j + 1] = cc;
-            }
-            if (sp + nch > STACK) {
-                flag_error(A.err, DE_STACK);
-                return -1;
+                key[q + 1] = kk;
+                ch[q + 1] = cc;
             }
             for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
         } else {
-            if (nd.a < 0 || nd.b > A.n) {
+            if (nd_a < 0 || nd_b > A.n) {
                 guard_fail(A, 2, s, node);
                 return -2;
             }
-            for (int j = nd.a; j < nd.b; ++j) {
-                if (j == s) continue;
-                (void)SDOT_CHECK_IDX(j, A.n, 6);
-                const double c1x = A.pos[2 * j], c1y = A.pos[2 * j + 1], w1 = A.w[j];
-                double ox, oy, nx, ny;
-                bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
-                n = plane_cut(cell, n, cap, ox, oy, nx, ny, j, true);
-                if (n <= 0) return n;
-            }
+            j = nd_a;
+            je = nd_b;
         }
     }
     return n;
 }
 
-// Full per-cell work.  Returns false when a capacity was exceeded (the cell
-// is then rebuilt by the next tier, which rewrites every output of it).
+// Per-cell work once the polygon of Dirac s is built (n vertices; -1: a
+// capacity was exceeded, -2: a guard failed).  Returns false when a capacity
+// was exceeded (the cell is then rebuilt by the next tier, which rewrites
+// every output of it).
 template <int MODE, bool BALL>
-SDOT_KFN bool process_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double *acc,
-                             int acc_st, const PolyView<double> &piece, Out &row, Out &nbo) {
+SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int n, int cap, double *acc,
+                            int acc_st, const PolyView<double> &piece, Out &row, Out &nbo) {
     const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
-    const int n = build_cell(A, s, cell, cap, c0x, c0y, w0);
     if (n == -2) {
         // failed guard: report a NaN cell, not an overflow
         if (A.mass) A.mass[s] = nan("");
@@ -470,9 +507,10 @@ __global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
                            reinterpret_cast<int *>(extra + 3 * CAP * T2D) + t, T2D, CAP};
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
+    const int n = build_cell(A, s, cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s]);
     Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
     Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
-    if (process_cell<MODE, BALL>(A, s, cell, CAP, acc, T2D, piece, row, nbo)) {
+    if (finish_cell<MODE, BALL>(A, s, cell, n, CAP, acc, T2D, piece, row, nbo)) {
         if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
         if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
     } else {
@@ -481,35 +519,34 @@ __global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
     }
 }
 
-// Scratch layout of one large tier: `S` threads, polygon capacity `cap`.
-struct TierScratch {
+// Polygon, accumulators and row buffers of one warp of the warp tier,
+// contiguous (vertex k at index k) so that the lanes read 32 vertices at once.
+struct WarpScratch {
     PolyView<double> cell, piece;
-    double *acc;
-    int *row_col;
-    double *row_val;
-    int *nb_id;
-    SDOT_HDI TierScratch(double *base, long long S, int cap, int g) {
+    double *acc, *row_val;
+    int *row_col, *nb_id;
+    __device__ WarpScratch(double *base, int cap) {
         double *p = base;
-        cell = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S), cap};
-        p += 3 * cap * S;
-        acc = p + g;
-        p += cap * S;
-        piece = PolyView<double>{p + g, p + cap * S + g, reinterpret_cast<int *>(p + 2 * cap * S) + g, int(S), cap};
-        p += 3 * cap * S;
-        row_val = p + g;
-        p += (cap + 1) * S;
-        row_col = reinterpret_cast<int *>(p) + g;
-        p += (cap + 1) * S;
-        nb_id = reinterpret_cast<int *>(p) + g;
+        cell = PolyView<double>{p, p + cap, reinterpret_cast<int *>(p + 2 * cap), 1, cap};
+        p += 3 * cap;
+        acc = p;
+        p += cap;
+        piece = PolyView<double>{p, p + cap, reinterpret_cast<int *>(p + 2 * cap), 1, cap};
+        p += 3 * cap;
+        row_val = p;
+        p += cap + 1;
+        row_col = reinterpret_cast<int *>(p);
+        p += cap + 1;
+        nb_id = reinterpret_cast<int *>(p);  // 2 cap ints
     }
 };
-// doubles of one tier's scratch: cell (3 cap), acc (cap), piece (3 cap),
-// row values (cap + 1), row columns (cap + 1, ints in double slots), ids (2 cap ints)
-__host__ __device__ constexpr long long tier_doubles(long long S, int cap) {
-    return S * (7LL * cap + 2LL * (cap + 1) + 2LL * cap);
+// doubles of one warp's scratch: cell (3 cap), acc (cap), piece (3 cap), row
+// values (cap + 1), row columns (cap + 1), ids (2 cap ints), rounded up
+__host__ __device__ constexpr long long warp_scratch_doubles(int cap) {
+    return (8LL * cap + 2LL * (cap + 1) + 31) / 32 * 32;
 }
 
-// Copies a finished row from tier scratch to its ELL slot or the side buffer.
+// Copies a finished row from scratch to its ELL slot or the side buffer.
 __device__ bool commit(const Rows &R, long long s, const int *col, const double *val, long long st, int cnt) {
     if (cnt <= R.cap) {
         for (int k = 0; k < cnt; ++k) {
@@ -529,31 +566,132 @@ __device__ bool commit(const Rows &R, long long s, const int *col, const double 
     return true;
 }
 
-template <int MODE, bool BALL, int CAP>
-__global__ void __launch_bounds__(64) k_cells2d_tier(const Cell2DArgs A, double *scratch, int nthreads, const int *list,
-                                                     const int *list_cnt, int *next_list, int *next_cnt) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= nthreads) return;
-    TierScratch T(scratch, nthreads, CAP, g);
+// Warp-per-cell build of one large cell (all lanes, same s): the walk of
+// build_cell, with the eviction test and the plane cuts spread over the
+// lanes, 32 vertices at a time.
+__device__ int build_cell_coop(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double c0x,
+                               double c0y, double w0, int *wstack) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int n = A.start_n;
+    if (lane == 0) {
+        for (int k = 0; k < n; ++k) {
+            cell.X(k) = A.start_xy[2 * k];
+            cell.Y(k) = A.start_xy[2 * k + 1];
+            cell.I(k) = domain_id(k);
+        }
+        wstack[0] = 0;
+    }
+    __syncwarp();
+    int sp = 1;
+    for (int visits = 0; sp > 0; ++visits) {
+        if (visits > A.max_nodes) {
+            if (lane == 0) flag_error(A.err, DE_ITER);
+            return -1;
+        }
+        const int node = wstack[--sp];
+        __syncwarp();
+        const TreeNode<2> nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
+        bool need = false;
+        for (int base = 0; base < n; base += 32) {
+            const int k = base + lane;
+            bool fail = false;
+            if (k < n) {
+                const double px = cell.X(k), py = cell.Y(k);
+                const double qx = fmin(nd.hi[0], fmax(nd.lo[0], px));
+                const double qy = fmin(nd.hi[1], fmax(nd.lo[1], py));
+                const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
+                const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - nd.maxw;
+                fail = !(lhs <= rhs);
+            }
+            if (__any_sync(FULL, fail)) {
+                need = true;
+                break;
+            }
+        }
+        if (!need) continue;
+        if (nd.b < 0) {
+            const int first = nd.a, nch = -nd.b;
+            if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
+                if (lane == 0) guard_fail(A, 1, s, node);
+                return -2;
+            }
+            if (sp + nch > STACK) {
+                if (lane == 0) flag_error(A.err, DE_STACK);
+                return -1;
+            }
+            float key[4];
+            int ch[4];
+            for (int c = 0; c < nch; ++c) {
+                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
+                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
+                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
+                key[c] = float(mx * mx + my * my);
+                ch[c] = first + c;
+            }
+            for (int i = 1; i < nch; ++i) {  // farthest first
+                const float kk = key[i];
+                const int cc = ch[i];
+                int j = i - 1;
+                while (j >= 0 && key[j] < kk) {
+                    key[j + 1] = key[j];
+                    ch[j + 1] = ch[j];
+                    --j;
+                }
+                key[j + 1] = kk;
+                ch[j + 1] = cc;
+            }
+            if (lane == 0)
+                for (int c = 0; c < nch; ++c) wstack[sp + c] = ch[c];
+            __syncwarp();
+            sp += nch;
+        } else {
+            if (nd.a < 0 || nd.b > A.n) {
+                if (lane == 0) guard_fail(A, 2, s, node);
+                return -2;
+            }
+            for (int j = nd.a; j < nd.b; ++j) {
+                if (j == s) continue;
+                const double c1x = A.pos[2 * j], c1y = A.pos[2 * j + 1], w1 = A.w[j];
+                double ox, oy, nx, ny;
+                bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
+                n = plane_cut_warp(cell, n, cap, ox, oy, nx, ny, j, true);
+                if (n <= 0) return n;
+            }
+        }
+    }
+    return n;
+}
+
+// Cells that overflowed the fast tier: one warp per cell, polygon of up to
+// CAP_HUGE_2D vertices in global scratch; lane 0 integrates the built cell.
+template <int MODE, bool BALL>
+__global__ void __launch_bounds__(128) k_cells2d_wtier(const Cell2DArgs A, double *scratch, int nwarps,
+                                                       const int *list, const int *list_cnt) {
+    constexpr int CAP = CAP_HUGE_2D;
+    __shared__ int wstack[4][STACK];
+    const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+    const int gw = blockIdx.x * 4 + wb;
+    if (gw >= nwarps) return;
+    WarpScratch W(scratch + (long long)gw * warp_scratch_doubles(CAP), CAP);
     const int cnt = *list_cnt;
-    for (int i = g; i < cnt; i += nthreads) {
+    for (int i = gw; i < cnt; i += nwarps) {
         const long long s = list[i];
-        Out row(A.rows.cnt ? T.row_col : nullptr, T.row_val, nthreads, CAP + 1);
-        Out nbo(A.nb.cnt ? T.nb_id : nullptr, nullptr, nthreads, 2 * CAP);
-        bool ok = process_cell<MODE, BALL>(A, s, T.cell, CAP, T.acc, nthreads, T.piece, row, nbo);
-        if (ok && A.rows.cnt) ok = commit(A.rows, s, T.row_col, T.row_val, nthreads, row.cnt);
-        if (ok && A.nb.cnt) ok = commit(A.nb, s, T.nb_id, nullptr, nthreads, nbo.cnt);
-        if (!ok) {
-            if (next_list) {
-                const int k = atomicAdd(next_cnt, 1);
-                next_list[k] = int(s);
-            } else {
+        const int n = build_cell_coop(A, s, W.cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s], wstack[wb]);
+        if (lane == 0) {
+            Out row(A.rows.cnt ? W.row_col : nullptr, W.row_val, 1, CAP + 1);
+            Out nbo(A.nb.cnt ? W.nb_id : nullptr, nullptr, 1, 2 * CAP);
+            bool ok = finish_cell<MODE, BALL>(A, s, W.cell, n, CAP, W.acc, 1, W.piece, row, nbo);
+            if (ok && A.rows.cnt) ok = commit(A.rows, s, W.row_col, W.row_val, 1, row.cnt);
+            if (ok && A.nb.cnt) ok = commit(A.nb, s, W.nb_id, nullptr, 1, nbo.cnt);
+            if (!ok) {
                 atomicOr(A.err, DE_CAPACITY);
                 if (A.mass) A.mass[s] = nan("");
                 if (A.rows.cnt) A.rows.cnt[s] = 0;
                 if (A.nb.cnt) A.nb.cnt[s] = 0;
             }
         }
+        __syncwarp();
     }
 }
 
@@ -570,13 +708,8 @@ void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
     k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
-    double *scr = static_cast<double *>(scratch);
-    k_cells2d_tier<MODE, BALL, CAP_BIG_2D><<<ceil_div(BIG_THREADS, 64), 64, 0, st>>>(
-        a, scr, BIG_THREADS, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2);
-    note_launch();
-    SDOT_CUDA(cudaGetLastError());
-    k_cells2d_tier<MODE, BALL, CAP_HUGE_2D><<<ceil_div(HUGE_THREADS, 64), 64, 0, st>>>(
-        a, scr, HUGE_THREADS, a.ovf_list2, a.ovf_cnt2, nullptr, nullptr);
+    k_cells2d_wtier<MODE, BALL><<<WTIER_WARPS / 4, 128, 0, st>>>(a, static_cast<double *>(scratch), WTIER_WARPS,
+                                                                  a.ovf_list, a.ovf_cnt);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
@@ -592,14 +725,12 @@ void cells2d_read_checks(unsigned long long out[3]) {
 }
 
 size_t cells2d_scratch_bytes() {
-    const long long a = tier_doubles(BIG_THREADS, CAP_BIG_2D), b = tier_doubles(HUGE_THREADS, CAP_HUGE_2D);
-    return size_t(a > b ? a : b) * sizeof(double) + 256;
+    return size_t(warp_scratch_doubles(CAP_HUGE_2D)) * WTIER_WARPS * sizeof(double) + 256;
 }
 
 void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
     if (a.n == 0) return;
     SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
-    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt2, 0, sizeof(int), st));
     if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
     if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
     const bool ball = a.ball != 0;

@@ -7,16 +7,16 @@ namespace sdot {
 
 enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2 };
 
-// Cell polygon capacities of the three tiers.  Every cell is first built by
-// the fast kernel (polygon in shared memory); cells that overflow it are
-// rebuilt by the big tier, then by the huge tier (polygons in global scratch).
-// Beyond the huge capacity the call reports ST_CAPACITY.
+// Cell polygon capacities of the two tiers.  Every cell is first built by
+// the fast kernel (one thread per cell, polygon in shared memory); cells that
+// overflow it are rebuilt by the warp tier (one warp per cell, polygon in
+// global scratch).  Beyond the warp tier's capacity the call reports
+// ST_CAPACITY.
 constexpr int CAP_FAST_2D = 16;
-constexpr int CAP_BIG_2D = 64;
 constexpr int CAP_HUGE_2D = 1024;
 // Hessian rows and neighbour lists are stored slot-major (ELL) with these
-// widths; longer rows (only cells of the big / huge tiers) go to a side
-// buffer, their offset in row_side[s].
+// widths; longer rows (only cells of the warp tier) go to a side buffer,
+// their offset in Rows::side[s].
 constexpr int ROWCAP_2D = 24;
 constexpr int NBCAP_2D = 40;
 
@@ -69,11 +69,9 @@ struct Cell2DArgs {
     double *ctd = nullptr;        // 2n centroids
     Rows rows;                    // Hessian rows (rows.cnt null: skipped)
     Rows nb;                      // boundary ids of each cell (nb.cnt null: skipped)
-    // overflow handling (lists of sorted indices handed to the next tier)
+    // cells that overflow the fast tier (sorted indices handed to the warp tier)
     int *ovf_list = nullptr;
     int *ovf_cnt = nullptr;
-    int *ovf_list2 = nullptr;
-    int *ovf_cnt2 = nullptr;
     unsigned *err = nullptr;
     int *guard = nullptr;          // first failed guard: (code, sorted index, value)
     long long item_nv = 0;         // number of item vertices (multi items)

@@ -49,21 +49,40 @@ struct PolyView {
 // set the distances (and so the interpolation ratios) are divided by |nrm|
 // as the reference does for un-normalised normals (N<0>).
 // Returns the new vertex count, or -1 if the result would exceed `cap`.
-template <class T>
-SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize) {
-    // one pass gives every fact the reference reads from its `outside`
-    // bitset: count, first set bit, first clear bit, bits 1 and n - 1
+// The facts the reference reads from its `outside` bitset: count, first set
+// bit, first clear bit, bits 1 and n - 1 (one pass over the vertices).
+struct CutFacts {
     int nb_out = 0, first_out = -1, first_in = -1;
     bool out1 = false, out_last = false;
-    for (int k = 0; k < n; ++k) {
-        const T d = (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny;
-        const bool o = d < T(0);
+    SDOT_HD void add(int k, int n, bool o) {
         nb_out += o;
         if (o && first_out < 0) first_out = k;
         if (!o && first_in < 0) first_in = k;
         if (k == 1) out1 = o;
         if (k == n - 1) out_last = o;
     }
+};
+
+template <class T>
+SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize,
+                            const CutFacts &f);
+
+template <class T>
+SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize) {
+    CutFacts f;
+    for (int k = 0; k < n; ++k) {
+        const T d = (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny;
+        f.add(k, n, d < T(0));
+    }
+    return plane_cut_apply(p, n, cap, ox, oy, nx, ny, cut_id, normalize, f);
+}
+
+// The cut itself, given the classification of the vertices.
+template <class T>
+SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize,
+                            const CutFacts &f) {
+    const int nb_out = f.nb_out, first_out = f.first_out, first_in = f.first_in;
+    const bool out1 = f.out1, out_last = f.out_last;
     if (nb_out == 0) return n;
     if (nb_out == n) return 0;
     T inv = T(1);
@@ -143,6 +162,165 @@ SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T 
         return n - nb_rem;
     }
 }
+
+#ifdef __CUDACC__
+// plane_cut done by a whole warp on one polygon (all 32 lanes call it with the
+// same arguments): the lanes classify 32 vertices at a time, the facts the
+// scalar version gathers in its pass come from warp votes, and vertex moves
+// are done 32 at a time, each chunk read before it is written, in the order
+// that keeps the scalar loop's result.  Same cases, same new vertices, same
+// vertex order as plane_cut.
+template <class T>
+__device__ int plane_cut_warp(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id,
+                              bool normalize) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int nb_out = 0, first_out = -1, first_in = -1;
+    bool out1 = false, out_last = false;
+    for (int base = 0; base < n; base += 32) {
+        const int k = base + lane;
+        const bool valid = k < n;
+        bool o = false;
+        if (valid) {
+            const T d = (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny;
+            o = d < T(0);
+        }
+        const unsigned mo = __ballot_sync(FULL, o), mi = __ballot_sync(FULL, valid && !o);
+        nb_out += __popc(mo);
+        if (first_out < 0 && mo) first_out = base + __ffs(mo) - 1;
+        if (first_in < 0 && mi) first_in = base + __ffs(mi) - 1;
+        if (base == 0 && n > 1) out1 = (mo >> 1) & 1u;
+        if (n - 1 < base + 32) out_last = (mo >> (n - 1 - base)) & 1u;
+    }
+    if (nb_out == 0) return n;
+    if (nb_out == n) return 0;
+    T inv = T(1);
+    if (normalize) inv = T(1) / sqrt(nx * nx + ny * ny);
+    auto dist = [&](int k) -> T { return ((ox - p.X(k)) * nx + (oy - p.Y(k)) * ny) * inv; };
+    int i1 = first_out;
+    if (nb_out == 1) {
+        if (n + 1 > cap) return -1;
+        const int i0 = (i1 + n - 1) % n, i2 = (i1 + 1) % n;
+        const T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1), p2x = p.X(i2), p2y = p.Y(i2);
+        const T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2);
+        const T m0 = s0 / (s1 - s0), m1 = s2 / (s1 - s2);
+        const int id1 = p.I(i1);
+        __syncwarp();
+        for (int hi = n; hi > i1 + 1; hi -= 32) {  // [i1 + 1, n) moves up by one, top chunk first
+            const int lo = hi - 32 > i1 + 1 ? hi - 32 : i1 + 1;
+            const int k = lo + lane;
+            T vx = T(0), vy = T(0);
+            int vi = 0;
+            if (k < hi) {
+                vx = p.X(k);
+                vy = p.Y(k);
+                vi = p.I(k);
+            }
+            __syncwarp();
+            if (k < hi) {
+                p.X(k + 1) = vx;
+                p.Y(k + 1) = vy;
+                p.I(k + 1) = vi;
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            p.X(i1 + 1) = p2x - m1 * (p1x - p2x);
+            p.Y(i1 + 1) = p2y - m1 * (p1y - p2y);
+            p.I(i1 + 1) = id1;
+            p.X(i1) = p0x - m0 * (p1x - p0x);
+            p.Y(i1) = p0y - m0 * (p1y - p0y);
+            p.I(i1) = cut_id;
+        }
+        __syncwarp();
+        return n + 1;
+    }
+    if (nb_out == 2) {
+        if (i1 == 0 && !out1) i1 = n - 1;
+        const int i0 = (i1 + n - 1) % n, i2 = (i1 + 1) % n, i3 = (i1 + 2) % n;
+        const T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
+        const T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
+        const T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
+        const T m1 = s0 / (s1 - s0), m2 = s3 / (s2 - s3);
+        __syncwarp();
+        if (lane == 0) {
+            p.X(i1) = p0x - m1 * (p1x - p0x);
+            p.Y(i1) = p0y - m1 * (p1y - p0y);
+            p.I(i1) = cut_id;
+            p.X(i2) = p3x - m2 * (p2x - p3x);
+            p.Y(i2) = p3y - m2 * (p2y - p3y);
+        }
+        __syncwarp();
+        return n;
+    }
+    // left move of [src0, src0 + cnt) to [src0 - by, ...), low chunk first
+    auto move_down = [&](int src0, int cnt, int by) {
+        for (int c = 0; c < cnt; c += 32) {
+            const int k = src0 + c + lane;
+            const bool v = c + lane < cnt;
+            T vx = T(0), vy = T(0);
+            int vi = 0;
+            if (v) {
+                vx = p.X(k);
+                vy = p.Y(k);
+                vi = p.I(k);
+            }
+            __syncwarp();
+            if (v) {
+                p.X(k - by) = vx;
+                p.Y(k - by) = vy;
+                p.I(k - by) = vi;
+            }
+            __syncwarp();
+        }
+    };
+    if (i1 == 0 && out_last) {
+        const int nb_in = n - nb_out;
+        const int i3 = first_in;
+        i1 = nb_in + i3;
+        const int i0 = i1 - 1, i2 = i3 - 1;
+        const T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
+        const T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
+        const T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
+        const T m1 = s0 / (s1 - s0), m2 = s3 / (s2 - s3);
+        const int id2 = p.I(i2);
+        __syncwarp();
+        if (lane == 0) {
+            p.X(0) = p3x - m2 * (p2x - p3x);
+            p.Y(0) = p3y - m2 * (p2y - p3y);
+            p.I(0) = id2;
+        }
+        __syncwarp();
+        if (i2 > 0) move_down(i2 + 1, nb_in, i2);
+        if (lane == 0) {
+            p.X(nb_in + 1) = p0x - m1 * (p1x - p0x);
+            p.Y(nb_in + 1) = p0y - m1 * (p1y - p0y);
+            p.I(nb_in + 1) = cut_id;
+        }
+        __syncwarp();
+        return nb_in + 2;
+    }
+    const int i0 = (i1 + n - 1) % n, i2 = (i1 + nb_out - 1) % n, i3 = (i1 + nb_out) % n;
+    const T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
+    const T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
+    const T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
+    const T m1 = s0 / (s1 - s0), m2 = s3 / (s2 - s3);
+    const int id2 = p.I(i2);
+    __syncwarp();
+    if (lane == 0) {
+        p.X(i1) = p0x - m1 * (p1x - p0x);
+        p.Y(i1) = p0y - m1 * (p1y - p0y);
+        p.I(i1) = cut_id;
+        p.X(i1 + 1) = p3x - m2 * (p2x - p3x);
+        p.Y(i1 + 1) = p3y - m2 * (p2y - p3y);
+        p.I(i1 + 1) = id2;
+    }
+    __syncwarp();
+    const int nb_rem = nb_out - 2;
+    if (i2 + 1 < n) move_down(i2 + 1, n - i2 - 1, nb_rem);
+    return n - nb_rem;
+}
+#endif
 
 // Weighted bisector of (c0, w0) and (c1, w1) as the reference's traversal
 // builds it (src/sdot/PowerDiagram/Visitors/SpZGrid.tcc:506-522): origin

@@ -29,24 +29,46 @@ __device__ double block_sum(double v, double *sh) {
     return r;  // valid in thread 0
 }
 
-__device__ double row_dot(const Rows &R, long long s, const double *x) {
-    const int m = R.cnt[s];
-    double acc = 0;
-    if (m <= R.cap) {
-        for (int k = 0; k < m; ++k) acc += R.val[k * R.stride + s] * x[R.col[k * R.stride + s]];
-    } else {
-        const long long o = R.side[s];
-        for (int k = 0; k < m; ++k) acc += R.side_val[o + k] * x[R.side_col[o + k]];
-    }
-    return acc;
-}
-
-__global__ void k_diag_inv(Rows R, long long n, long long g, double *dinv, double *scal) {
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+// Matrix views for the PCG kernels: row s times x, and the diagonal entry.
+struct RowsMat {
+    Rows R;
+    __device__ double row_dot(long long s, const double *x) const {
         const int m = R.cnt[s];
+        double acc = 0;
+        if (m <= R.cap) {
+            for (int k = 0; k < m; ++k) acc += R.val[k * R.stride + s] * x[R.col[k * R.stride + s]];
+        } else {
+            const long long o = R.side[s];
+            for (int k = 0; k < m; ++k) acc += R.side_val[o + k] * x[R.side_col[o + k]];
+        }
+        return acc;
+    }
+    __device__ double diag(long long s) const {
         double d = 0;
-        for (int k = 0; k < m; ++k)
+        for (int k = 0, m = R.cnt[s]; k < m; ++k)
             if (*R.colp(s, k) == s) d += *R.valp(s, k);
+        return d;
+    }
+};
+struct CsrView {
+    CsrMat M;
+    __device__ double row_dot(long long s, const double *x) const {
+        double acc = 0;
+        for (long long k = M.off[s], e = M.off[s + 1]; k < e; ++k) acc += M.val[k] * x[M.col[k]];
+        return acc;
+    }
+    __device__ double diag(long long s) const {
+        double d = 0;
+        for (long long k = M.off[s], e = M.off[s + 1]; k < e; ++k)
+            if (M.col[k] == s) d += M.val[k];
+        return d;
+    }
+};
+
+template <class M>
+__global__ void k_diag_inv(M A, long long n, long long g, double *dinv, double *scal) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        double d = A.diag(s);
         if (s == g) {
             scal[S_GDIAG] = d;
             d *= 2;
@@ -107,12 +129,13 @@ __global__ void k_final(const double *partial, int nb, double *scal, int mode) {
     }
 }
 
-__global__ void k_spmv(Rows R, long long n, long long g, const double *p, double *q, const double *scal,
+template <class M>
+__global__ void k_spmv(M A, long long n, long long g, const double *p, double *q, const double *scal,
                        double *partial) {
     __shared__ double sh[32];
     double pq = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-        double v = row_dot(R, s, p);
+        double v = A.row_dot(s, p);
         if (s == g) v += scal[S_GDIAG] * p[s];
         q[s] = v;
         pq += p[s] * v;
@@ -234,15 +257,18 @@ void pcg_bind(PcgWork &w, double *base, long long n) {
     w.scal = w.partial + 6 * PCG_BLOCKS;
 }
 
-PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                    int max_iter, const PcgWork &w, cudaStream_t st, int check) {
+namespace {
+
+template <class M>
+PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
+                  int max_iter, const PcgWork &w, cudaStream_t st, int check) {
     PcgResult res;
     if (n <= 0) {
         res.converged = true;
         return res;
     }
     const int g = grid_of(n);
-    k_diag_inv<<<g, TB, 0, st>>>(rows, n, gauge_row, w.dinv, w.scal);
+    k_diag_inv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.dinv, w.scal);
     note_launch();
     k_init<<<g, TB, 0, st>>>(b, x, w.r, w.z, w.p, w.dinv, w.partial, n);
     note_launch();
@@ -262,7 +288,7 @@ PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const do
     while (it < max_iter) {
         const int chunk = check < max_iter - it ? check : max_iter - it;
         for (int c = 0; c < chunk; ++c) {
-            k_spmv<<<g, TB, 0, st>>>(rows, n, gauge_row, w.p, w.q, w.scal, w.partial);
+            k_spmv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.p, w.q, w.scal, w.partial);
             note_launch();
             k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 1);
             note_launch();
@@ -287,6 +313,18 @@ PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const do
     res.rel_residual = std::sqrt(hs[S_RR] / rr0);
     if (res.rel_residual <= rel_tol) res.converged = true;
     return res;
+}
+
+}  // namespace
+
+PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
+                    int max_iter, const PcgWork &w, cudaStream_t st, int check) {
+    return pcg_run(RowsMat{rows}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check);
+}
+
+PcgResult pcg_solve_csr(const CsrMat &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
+                        int max_iter, const PcgWork &w, cudaStream_t st, int check) {
+    return pcg_run(CsrView{A}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check);
 }
 
 void mass_errors(const double *m, const double *t, long long n, double *partial, double *out, cudaStream_t st) {

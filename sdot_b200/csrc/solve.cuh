@@ -36,6 +36,15 @@ struct PcgResult {
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
                     int max_iter, const PcgWork &w, cudaStream_t st, int check = 32);
 
+// The same solve on a CSR matrix (device arrays: off[n + 1], col[nnz], val[nnz]).
+struct CsrMat {
+    const long long *off = nullptr;
+    const long long *col = nullptr;
+    const double *val = nullptr;
+};
+PcgResult pcg_solve_csr(const CsrMat &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
+                        int max_iter, const PcgWork &w, cudaStream_t st, int check = 32);
+
 // Device reductions used by the Newton loop (deterministic order).
 // out[0] = max_i |m_i - t_i| / t_i, out[1] = min_i m_i, out[2] = sum_i (m_i - t_i)^2
 void mass_errors(const double *m, const double *t, long long n, double *partial, double *out, cudaStream_t st);

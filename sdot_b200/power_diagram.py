@@ -207,3 +207,25 @@ class PowerDiagram:
         c = ctypes.c_int64(0)
         self._lib.sdot_last_overflow_count(self._ctx, ctypes.byref(c))
         return c.value
+
+
+def csr_solve(offsets, columns, values, b, gauge_fix=True, rel_tol=1e-12, max_iter=20000):
+    """Solves H x = b for a CSR matrix on the device (EigenSolver::solve,
+    EigenSolver.cpp:9-41, by Jacobi-preconditioned conjugate gradients).
+    Returns (x, iterations, relative residual); raises SdotError on failure."""
+    lib = _lib.load()
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    col = np.ascontiguousarray(columns, dtype=np.int64)
+    val = _f64(values)
+    rhs = _f64(b)
+    n = rhs.shape[0]
+    x = np.zeros(n)
+    it = ctypes.c_int64(0)
+    res = ctypes.c_double(0)
+    msg = ctypes.create_string_buffer(512)
+    st = lib.sdot_csr_solve(_ptr(off), _ptr(col), _ptr(val), n, _ptr(rhs), _ptr(x), int(bool(gauge_fix)),
+                            float(rel_tol), int(max_iter), SDOT_HOST, ctypes.byref(it), ctypes.byref(res), msg,
+                            len(msg))
+    if st != _lib.SDOT_OK:
+        raise SdotError(st, msg.value.decode())
+    return x, it.value, res.value

@@ -54,7 +54,8 @@ def test_newton_clustered(gpu_lib, ref_oracle):
     rng = np.random.default_rng(11)
     n = 5000
     p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng)])
-    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, p, np.zeros(n), np.full(n, 1.0 / n))
+    # tight clusters: the reachable relative mass error is ~7e-12 (CPU oracle)
+    gpu, w_g, w_r, rep, rep_r = solve_pair(ref_oracle, p, np.zeros(n), np.full(n, 1.0 / n), tol=2e-11)
     check_weights(w_g, w_r)
 
 
@@ -107,3 +108,25 @@ def test_void_start_rejected_by_damped_newton(gpu_lib):
     with pytest.raises(SdotError) as e:
         g.solve_weights(np.full(20_000, 1 / 20_000))
     assert e.value.status == SDOT_VOID_CELL
+
+
+def test_csr_solve_matches_direct_solve(gpu_lib, ref_oracle):
+    # the linear step alone: the reference CSR of C1 with the gauge fix,
+    # device conjugate gradients vs a direct sparse solve
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    from sdot_b200.power_diagram import csr_solve
+
+    c = workloads.config1()
+    n = len(c["weights"])
+    ref = ref_oracle.RefPowerDiagram(c["positions"], c["weights"])
+    ref.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    err, off, col, val, m = ref.der_integrals_wrt_weights()
+    b = m - 1.0 / n + np.random.default_rng(3).normal(0, 1e-6, n)
+    x, it, res = csr_solve(off, col, val, b, gauge_fix=True, rel_tol=1e-13)
+    v2 = val.copy()
+    v2[0] *= 2
+    x_ref = spla.spsolve(sp.csr_matrix((v2, col, off), shape=(n, n)).tocsc(), b)
+    assert res <= 1e-13
+    assert np.abs(x - x_ref).max() <= 1e-8 * np.abs(x_ref).max()
