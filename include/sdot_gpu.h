@@ -173,6 +173,30 @@ int sdot_csr_solve(const int64_t *offsets, const int64_t *columns, const double 
                    const double *b, double *x, int gauge_fix, double rel_tol, int max_iter, int mem_space,
                    int64_t *iterations, double *rel_residual, char *errbuf, int64_t errbuf_len);
 
+/* Allocation-free variant of sdot_csr_solve.  No reference counterpart.
+ *
+ * Meant for callers that cannot allocate device memory while they solve: a
+ * process whose free device memory is held by another allocator (a
+ * framework's caching allocator, say) would see an allocation fail or split
+ * that pool, and a latency-bound loop running one small solve per step cannot
+ * afford the device-wide synchronisation that cudaMalloc and cudaFree bring
+ * on every call.  The work vectors live in a fixed array compiled into the
+ * library (2.65 MB of device memory on each device), hence:
+ *   - n may not exceed SDOT_NOALLOC_MAX_ROWS; a larger n returns SDOT_BAD_ARG
+ *     with the limit in errbuf, before anything runs;
+ *   - offsets, columns, values, b and x are DEVICE pointers; stream is a
+ *     cudaStream_t (NULL: the default stream); the call returns once the
+ *     solve has finished on that stream;
+ *   - the first call on each device looks up that device's scratch array
+ *     (cudaGetSymbolAddress, with the device current), so make the first call
+ *     on a device before any stream capture on that device;
+ *   - calls whose work overlaps on one device (several threads or streams)
+ *     race on the shared scratch: the caller serialises them.
+ * Other arguments and results as sdot_csr_solve.                            */
+#define SDOT_NOALLOC_MAX_ROWS 65536
+int sdot_csr_solve_noalloc(const int64_t *offsets, const int64_t *columns, const double *values, int64_t n,
+                           const double *b, double *x, int gauge_fix, double rel_tol, int max_iter, void *stream,
+                           int64_t *iterations, double *rel_residual, char *errbuf, int64_t errbuf_len);
 
 /* Fused evaluation only, results kept on the device (for timing). */
 int sdot_evaluate(sdot_ctx *ctx);

@@ -83,6 +83,8 @@ SIGNATURES = {
     "sdot_get_weights": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "sdot_csr_solve": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                       ctypes.c_int, _P, _P, ctypes.c_char_p, _I64]),
+    "sdot_csr_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                              _P, _P, _P, ctypes.c_char_p, _I64]),
     "sdot_evaluate": (ctypes.c_int, [_P]),
     "sdot_last_timings": (ctypes.c_int, [_P, _P]),
     "sdot_last_overflow_count": (ctypes.c_int, [_P, _P]),

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsdot_b200.so")
-SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "csr.cu", "solve.cu", "api.cu", "peaks.cu"]
+SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "csr.cu", "solve.cu", "api.cu", "peaks.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
