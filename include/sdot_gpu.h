@@ -36,7 +36,8 @@ typedef enum sdot_status {
     SDOT_OOM = 5,
     SDOT_BAD_ARG = 6,
     SDOT_CUDA_ERROR = 7,
-    SDOT_UNSUPPORTED = 8
+    SDOT_UNSUPPORTED = 8,
+    SDOT_PENDING = 9          /* a served request is still queued or running */
 } sdot_status;
 
 enum { SDOT_HOST = 0, SDOT_DEVICE = 1 };
@@ -197,6 +198,44 @@ int sdot_csr_solve(const int64_t *offsets, const int64_t *columns, const double 
 int sdot_csr_solve_noalloc(const int64_t *offsets, const int64_t *columns, const double *values, int64_t n,
                            const double *b, double *x, int gauge_fix, double rel_tol, int max_iter, void *stream,
                            int64_t *iterations, double *rel_residual, char *errbuf, int64_t errbuf_len);
+
+/* ---- serving: continuously batched solves ---------------------------------
+ * No single reference counterpart: each request is one
+ * OptimalTransportSolver::solve (positions, starting weights, target masses,
+ * unit-density box domain).  A server runs `slots` requests at once, each on
+ * its own worker, contexts and CUDA stream (grids, weights, Hessian rows and
+ * solver buffers stay resident on the device and are reused); requests are
+ * admitted in arrival order as soon as a slot is free and the estimated
+ * device memory of the requests in flight fits hbm_budget_bytes (a request
+ * larger than the budget runs alone).  The device work of requests in flight
+ * overlaps.  slots = 1 runs the same solves one after the other.            */
+typedef struct sdot_server sdot_server;
+typedef struct sdot_server_opts {
+    int slots;                 /* requests in flight at once (1..64) */
+    int64_t hbm_budget_bytes;  /* admission budget for the requests in flight */
+    int device;                /* CUDA device; -1 -> current */
+    sdot_newton_opts newton;   /* per-request Newton options */
+} sdot_server_opts;
+typedef struct sdot_request_report {
+    int status;                /* SDOT_PENDING until done, then the solve's status */
+    double submit_ms, start_ms, end_ms;  /* since the server was created */
+    int iterations;            /* Newton iterations */
+    double max_rel_mass_error;
+} sdot_request_report;
+
+sdot_server *sdot_server_create(const sdot_server_opts *opts);
+/* Copies the inputs: positions double[n * dim], weights double[n] (NULL:
+ * zeros), target double[n], box corners double[dim] (NULL: unit box).
+ * Returns the request id (>= 0) or minus a status.                          */
+int64_t sdot_server_submit(sdot_server *srv, int dim, int64_t n, const double *positions, const double *weights,
+                           const double *target, const double *box_lo, const double *box_hi);
+/* SDOT_PENDING while the request is queued or running; then its status, the
+ * solved weights in weights_out (double[n], may be NULL) and its report.    */
+int sdot_server_poll(sdot_server *srv, int64_t id, double *weights_out, sdot_request_report *report);
+/* Blocks until every submitted request is done. */
+int sdot_server_drain(sdot_server *srv);
+/* Finishes the requests still queued, then stops the workers. */
+void sdot_server_destroy(sdot_server *srv);
 
 /* Fused evaluation only, results kept on the device (for timing). */
 int sdot_evaluate(sdot_ctx *ctx);

@@ -20,8 +20,9 @@ SDOT_OOM = 5
 SDOT_BAD_ARG = 6
 SDOT_CUDA_ERROR = 7
 SDOT_UNSUPPORTED = 8
+SDOT_PENDING = 9
 STATUS_NAMES = {0: "OK", 1: "VOID_CELL", 2: "CAPACITY", 3: "NOT_CONVERGED", 4: "ITER_CAP", 5: "OOM",
-                6: "BAD_ARG", 7: "CUDA_ERROR", 8: "UNSUPPORTED"}
+                6: "BAD_ARG", 7: "CUDA_ERROR", 8: "UNSUPPORTED", 9: "PENDING"}
 
 SDOT_HOST = 0
 SDOT_DEVICE = 1
@@ -55,6 +56,16 @@ class SdotNewtonReport(ctypes.Structure):
     ]
 
 
+class SdotServerOptions(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64), ("device", ctypes.c_int),
+                ("newton", SdotNewtonOptions)]
+
+
+class SdotRequestReport(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("submit_ms", ctypes.c_double), ("start_ms", ctypes.c_double),
+                ("end_ms", ctypes.c_double), ("iterations", ctypes.c_int), ("max_rel_mass_error", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
 _I64 = ctypes.c_int64
@@ -85,6 +96,11 @@ SIGNATURES = {
                                       ctypes.c_int, _P, _P, ctypes.c_char_p, _I64]),
     "sdot_csr_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                               _P, _P, _P, ctypes.c_char_p, _I64]),
+    "sdot_server_create": (_P, [ctypes.POINTER(SdotServerOptions)]),
+    "sdot_server_submit": (_I64, [_P, ctypes.c_int, _I64, _P, _P, _P, _P, _P]),
+    "sdot_server_poll": (ctypes.c_int, [_P, _I64, _P, ctypes.POINTER(SdotRequestReport)]),
+    "sdot_server_drain": (ctypes.c_int, [_P]),
+    "sdot_server_destroy": (None, [_P]),
     "sdot_evaluate": (ctypes.c_int, [_P]),
     "sdot_last_timings": (ctypes.c_int, [_P, _P]),
     "sdot_last_overflow_count": (ctypes.c_int, [_P, _P]),

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsdot_b200.so")
-SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "csr.cu", "solve.cu", "api.cu", "peaks.cu", "noalloc.cu"]
+SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "cell3d.cu", "csr.cu", "solve.cu", "api.cu", "server.cu", "peaks.cu",
+           "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

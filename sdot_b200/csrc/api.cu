@@ -1,6 +1,7 @@
 // C ABI of libsdot_b200.so (include/sdot_gpu.h): context, domain, evaluation.
 #include "../../include/sdot_gpu.h"
 #include "cell2d.cuh"
+#include "cell3d.cuh"
 #include "csr.cuh"
 #include "geom2d.cuh"
 #include "prims.cuh"
@@ -95,10 +96,18 @@ struct sdot_ctx {
     long long n = 0, cap = 0;
     double *d_pos = nullptr, *d_w = nullptr;
     DeviceTree<2> tree2;
+    DeviceTree<3> tree3;
+    // sorted -> caller order and its inverse, of the tree of this dimension
+    const int *perm() const { return dim == 3 ? tree3.idx : tree2.idx; }
+    const int *perm_inv() const { return dim == 3 ? tree3.inv : tree2.inv; }
     bool pos_dirty = true, w_dirty = true, dom_dirty = true, eval_dirty = true, nb_dirty = true;
 
     // domain (host side)
     std::vector<Item2> items;
+    struct Box3 {
+        double lo[3], hi[3], coeff;
+    };
+    std::vector<Box3> boxes3;  // 3D domain: boxes (one supported)
     bool has_image = false;
     double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};
     long long img_size[2] = {0, 0};
@@ -135,6 +144,7 @@ struct sdot_ctx {
     ~sdot_ctx() {
         cudaSetDevice(device);
         tree2.release();
+        tree3.release();
         dfree(d_pos); dfree(d_w);
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
         free_eval();
@@ -181,9 +191,9 @@ struct sdot_ctx {
         if (ecap >= n && s_mass) return;
         free_eval();
         ecap = std::max<long long>(n, 1);
-        dalloc(s_mass, ecap); dalloc(s_mass_c, ecap); dalloc(s_ctd, 2 * ecap);
-        dalloc(o_mass, ecap); dalloc(o_mass_c, ecap); dalloc(o_ctd, 2 * ecap);
-        alloc_rows(rows, ecap, ROWCAP_2D, true);
+        dalloc(s_mass, ecap); dalloc(s_mass_c, ecap); dalloc(s_ctd, size_t(dim) * ecap);
+        dalloc(o_mass, ecap); dalloc(o_mass_c, ecap); dalloc(o_ctd, size_t(dim) * ecap);
+        alloc_rows(rows, ecap, dim == 3 ? ROWCAP_3D : ROWCAP_2D, true);
         dalloc(cnt_orig, ecap + 1);
         dalloc(offsets, ecap + 1);
         dalloc(ovf_list, ecap);
@@ -264,6 +274,7 @@ struct sdot_ctx {
         a.start_xy = d_start;
         a.coeff = coeff;
         a.mode = mode;
+        a.mixed = precision == SDOT_MIXED;
         a.ball = ball;
         a.img_lo[0] = img_lo[0]; a.img_lo[1] = img_lo[1];
         a.img_hi[0] = img_hi[0]; a.img_hi[1] = img_hi[1];
@@ -281,25 +292,63 @@ struct sdot_ctx {
         return a;
     }
 
+    // the domain is one the kernels handle; uploads the 2D one
+    void check_domain() {
+        if (dim == 3) {
+            if (boxes3.size() != 1)
+                throw Unsupported(boxes3.empty() ? "no domain: call sdot_add_box_shape first"
+                                                 : "3D domains of several boxes are not available in this build");
+            if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
+            return;
+        }
+        upload_domain();
+        if (mode == DM_MULTI)
+            throw Unsupported("domains made of several shapes are not enabled in this build (the multi-shape "
+                              "cell kernel is disabled); use one shape or an image density");
+    }
+
+    Cell3DArgs args3() {
+        Cell3DArgs a;
+        a.n = n;
+        a.pos = tree3.pos;
+        a.w = tree3.w;
+        a.nodes = tree3.nodes;
+        a.max_nodes = tree3.max_nodes;
+        for (int d = 0; d < 3; ++d) {
+            a.box_lo[d] = boxes3[0].lo[d];
+            a.box_hi[d] = boxes3[0].hi[d];
+        }
+        a.coeff = boxes3[0].coeff;
+        a.ovf_list = ovf_list;
+        a.ovf_cnt = ovf_cnt;
+        a.err = err;
+        a.guard = guard;
+        return a;
+    }
+
     void ensure_tree() {
         if (n == 0) throw BadArg("no Diracs: call sdot_set_diracs first");
         if (pos_dirty) {
-            tree2.max_per_leaf = int(max_per_leaf);
-            tree2.build(d_pos, d_w, n, stream);
+            if (dim == 3) {
+                tree3.max_per_leaf = int(max_per_leaf);
+                tree3.build(d_pos, d_w, n, stream);
+            } else {
+                tree2.max_per_leaf = int(max_per_leaf);
+                tree2.build(d_pos, d_w, n, stream);
+            }
             pos_dirty = w_dirty = false;
         } else if (w_dirty) {
-            tree2.update_weights(d_w, stream);
+            if (dim == 3)
+                tree3.update_weights(d_w, stream);
+            else
+                tree2.update_weights(d_w, stream);
             w_dirty = false;
         }
     }
 
     int evaluate() {
         if (!eval_dirty) return finish_status();
-        if (dim != 2) throw Unsupported("dim 3 is not available in this build");
-        upload_domain();
-        if (mode == DM_MULTI)
-            throw Unsupported("domains made of several shapes are not enabled in this build (the multi-shape "
-                              "cell kernel is disabled); use one shape or an image density");
+        check_domain();
         reserve_eval();
         if (!ev[0]) for (auto &e : ev) SDOT_CUDA(cudaEventCreate(&e));
         SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
@@ -307,18 +356,28 @@ struct sdot_ctx {
         SDOT_CUDA(cudaEventRecord(ev[0], stream));
         ensure_tree();
         SDOT_CUDA(cudaEventRecord(ev[1], stream));
-        Cell2DArgs a = args();
-        a.mass = s_mass;
-        a.mass_c = s_mass_c;
-        a.ctd = s_ctd;
-        a.rows = rows;
-        cells2d_launch(a, scratch, stream);
+        if (dim == 3) {
+            Cell3DArgs a = args3();
+            a.mass = s_mass;
+            a.ctd = s_ctd;
+            a.rows = rows;
+            cells3d_launch(a, stream);
+            // get_centroids' mass is the integral itself in 3D
+            SDOT_CUDA(cudaMemcpyAsync(s_mass_c, s_mass, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        } else {
+            Cell2DArgs a = args();
+            a.mass = s_mass;
+            a.mass_c = s_mass_c;
+            a.ctd = s_ctd;
+            a.rows = rows;
+            cells2d_launch(a, scratch, stream);
+        }
         SDOT_CUDA(cudaEventRecord(ev[2], stream));
-        csr_sort_merge(rows, n, tree2.idx, cnt_orig, stream);
+        csr_sort_merge(rows, n, perm(), cnt_orig, stream);
         scan_exclusive_total<long long>(cnt_orig, offsets, n, scan_tmp, stream);
-        unpermute(s_mass, o_mass, n, 1, tree2.idx, stream);
-        unpermute(s_mass_c, o_mass_c, n, 1, tree2.idx, stream);
-        unpermute(s_ctd, o_ctd, n, 2, tree2.idx, stream);
+        unpermute(s_mass, o_mass, n, 1, perm(), stream);
+        unpermute(s_mass_c, o_mass_c, n, 1, perm(), stream);
+        unpermute(s_ctd, o_ctd, n, dim, perm(), stream);
         SDOT_CUDA(cudaEventRecord(ev[3], stream));
         SDOT_CUDA(cudaMemcpyAsync(&nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaMemcpyAsync(&last_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
@@ -338,7 +397,13 @@ struct sdot_ctx {
             return SDOT_ITER_CAP;
         }
         if (last_err & DE_CAPACITY) {
-            last_error = "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
+            last_error = dim == 3 ? "a cell exceeded the maximum polyhedron capacity (64 faces of 32 vertices) or "
+                                    "the long-row buffer"
+                                  : "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
+            return SDOT_CAPACITY;
+        }
+        if (last_err & DE_DEGEN) {
+            last_error = "a 3D cut met degenerate geometry (the affected cells are NaN)";
             return SDOT_CAPACITY;
         }
         if (last_err & DE_GUARD) {
@@ -356,13 +421,19 @@ struct sdot_ctx {
     void evaluate_neighbors() {
         if (!nb_dirty) return;
         evaluate();
-        if (!nb.cnt || nb.stride < ecap) alloc_rows(nb, ecap, NBCAP_2D, false);
+        if (!nb.cnt || nb.stride < ecap) alloc_rows(nb, ecap, dim == 3 ? NBCAP_3D : NBCAP_2D, false);
         if (!nb_offsets) dalloc(nb_offsets, ecap + 1);
         SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
-        Cell2DArgs a = args();
-        a.nb = nb;
-        cells2d_launch(a, scratch, stream);
-        nb_counts(nb, n, tree2.idx, cnt_orig, stream);
+        if (dim == 3) {
+            Cell3DArgs a = args3();
+            a.nb = nb;
+            cells3d_launch(a, stream);
+        } else {
+            Cell2DArgs a = args();
+            a.nb = nb;
+            cells2d_launch(a, scratch, stream);
+        }
+        nb_counts(nb, n, perm(), cnt_orig, stream);
         scan_exclusive_total<long long>(cnt_orig, nb_offsets, n, scan_tmp, stream);
         SDOT_CUDA(cudaMemcpyAsync(&nb_total, nb_offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaStreamSynchronize(stream));
@@ -419,7 +490,7 @@ struct sdot_ctx {
         ++rep.evaluations;
         if (st != SDOT_OK) return st;
         // targets in sorted (tree) order; the order is fixed while the positions are
-        gather_sorted(t_orig, tree2.idx, t_sorted, n, stream);
+        gather_sorted(t_orig, perm(), t_sorted, n, stream);
         double et[3];
         mass_stats(t_sorted, et);  // et[1] = min target
         if (!(et[1] > 0)) throw BadArg("target masses must be positive");
@@ -427,7 +498,7 @@ struct sdot_ctx {
         long long gauge = -1;
         if (!ball) {
             int g = 0;
-            SDOT_CUDA(cudaMemcpyAsync(&g, tree2.inv, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            SDOT_CUDA(cudaMemcpyAsync(&g, perm_inv(), sizeof(int), cudaMemcpyDeviceToHost, stream));
             SDOT_CUDA(cudaStreamSynchronize(stream));
             gauge = g;
         }
@@ -463,7 +534,8 @@ struct sdot_ctx {
             }
             SDOT_CUDA(cudaMemcpyAsync(w_old, d_w, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
             axpby(s_mass, t_sorted, rhs, 1.0, -1.0, n, stream);  // v_values -= masses (.tcc:89-90)
-            const PcgResult pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream);
+            const PcgResult pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream, 32,
+                                           stream != nullptr);
             rep.pcg_iterations += pr.iterations;
             if (o.verbosity > 0)
                 fprintf(stderr, "sdot newton %d: pcg %d iterations, relative residual %.3e\n", it, pr.iterations,
@@ -471,7 +543,7 @@ struct sdot_ctx {
             double tau = 1.0, en[3];
             bool accepted = false;
             for (int k = 0; k <= 40; ++k) {
-                apply_step(w_old, dir, tree2.idx, tau, d_w, n, stream);  // weights -= dw (.tcc:106-109)
+                apply_step(w_old, dir, perm(), tau, d_w, n, stream);  // weights -= dw (.tcc:106-109)
                 set_device_weights_changed();
                 st = evaluate();
                 ++rep.evaluations;
@@ -618,9 +690,13 @@ int sdot_set_weights(sdot_ctx *ctx, const double *weights, int mem_space) {
 int sdot_add_box_shape(sdot_ctx *ctx, const double *p0, const double *p1, double coeff) {
     return guarded(ctx, [&] {
         if (!p0 || !p1) throw BadArg("null box corner");
-        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
         ctx->has_image = false;
-        ctx->items.push_back(box_item(p0[0], p0[1], p1[0], p1[1], coeff));
+        if (ctx->dim == 3) {
+            sdot_ctx::Box3 b{{p0[0], p0[1], p0[2]}, {p1[0], p1[1], p1[2]}, coeff};
+            ctx->boxes3.push_back(b);
+        } else {
+            ctx->items.push_back(box_item(p0[0], p0[1], p1[0], p1[1], coeff));
+        }
         ctx->dom_dirty = true;
         ctx->mark_dirty();
         return int(SDOT_OK);
@@ -631,7 +707,7 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
                                      double coeff) {
     return guarded(ctx, [&] {
         if (m <= 0 || !points || !normals) throw BadArg("bad convex polyhedron");
-        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
         // ConvexPolyhedronAssembly::add_convex_polyhedron: the bounding box of
         // the points inflated by its size, cut by each (point, normal) half-plane.
         double mn[2], mx[2];
@@ -690,7 +766,7 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
 int sdot_add_simplex_shape(sdot_ctx *ctx, const double *pts, double coeff) {
     return guarded(ctx, [&] {
         if (!pts) throw BadArg("null simplex");
-        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
         // ConvexPolyhedron2( Simplex ) (ConvexPolyhedron2.tcc:19-60)
         double p[3][2] = {{pts[0], pts[1]}, {pts[2], pts[3]}, {pts[4], pts[5]}};
         double cx = 1.0 / 3 * (p[0][0] + p[1][0] + p[2][0]), cy = 1.0 / 3 * (p[0][1] + p[1][1] + p[2][1]);
@@ -726,7 +802,7 @@ int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *ma
                            const int64_t *sizes, int nb_coeffs) {
     return guarded(ctx, [&] {
         if (!min_pt || !max_pt || !data || !sizes) throw BadArg("null image argument");
-        if (ctx->dim != 2) throw Unsupported("dim 3 is not available in this build");
+        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
         if (nb_coeffs != 1) throw Unsupported("only piecewise-constant images (nb_coeffs = 1) are available");
         if (sizes[0] <= 0 || sizes[1] <= 0) throw BadArg("bad image size");
         ctx->items.clear();
@@ -747,6 +823,7 @@ int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *ma
 int sdot_clear_domain(sdot_ctx *ctx) {
     return guarded(ctx, [&] {
         ctx->items.clear();
+        ctx->boxes3.clear();
         ctx->has_image = false;
         ctx->dom_dirty = true;
         ctx->mark_dirty();
@@ -765,6 +842,8 @@ static double domain_measure(const sdot_ctx *ctx) {
     }
     double res = 0;
     for (const Item2 &it : ctx->items) res += it.coeff * it.area();
+    for (const sdot_ctx::Box3 &b : ctx->boxes3)
+        res += b.coeff * (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
     return res;
 }
 
@@ -774,8 +853,10 @@ int sdot_normalize_domain(sdot_ctx *ctx) {
         if (mea != 0) {
             if (ctx->has_image)
                 for (double &v : ctx->img_data) v /= mea;
-            else
+            else {
                 for (Item2 &it : ctx->items) it.coeff /= mea;
+                for (sdot_ctx::Box3 &b : ctx->boxes3) b.coeff /= mea;
+            }
         }
         ctx->dom_dirty = true;
         ctx->mark_dirty();
@@ -847,7 +928,7 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
             dcols = tmp_c;
             dvals = tmp_v;
         }
-        csr_write(ctx->rows, n, ctx->tree2.idx, ctx->offsets, dcols, dvals, ctx->stream);
+        csr_write(ctx->rows, n, ctx->perm(), ctx->offsets, dcols, dvals, ctx->stream);
         if (mem_space != SDOT_DEVICE) {
             SDOT_CUDA(cudaMemcpyAsync(columns, tmp_c, nnz * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
             SDOT_CUDA(cudaMemcpyAsync(values, tmp_v, nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -890,7 +971,7 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
             dalloc(tmp, tot);
             dids = tmp;
         }
-        nb_write(ctx->nb, n, ctx->tree2.idx, ctx->nb_offsets, dids, ctx->stream);
+        nb_write(ctx->nb, n, ctx->perm(), ctx->nb_offsets, dids, ctx->stream);
         if (mem_space != SDOT_DEVICE)
             SDOT_CUDA(cudaMemcpyAsync(ids, tmp, tot * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
         ctx->copy_out(offsets, ctx->nb_offsets, size_t(n + 1) * sizeof(long long), mem_space);

@@ -75,10 +75,11 @@ struct Out {
 };
 
 // Integrates a streamed polygon (one piece at a time) and collects the
-// boundary measures for the Hessian row.
-template <bool DIRECT>
+// boundary measures for the Hessian row.  P: the cell's polygon view (its
+// ids name the neighbours).
+template <bool DIRECT, class P = PolyView<double>>
 struct Sink {
-    const PolyView<double> &cell;
+    const P &cell;
     const double *pos;
     double c0x, c0y, sqw0;
     double cx, cy, r;
@@ -97,8 +98,8 @@ struct Sink {
     Out &row;
     long long n_diracs = 1LL << 40;
 
-    SDOT_HDI Sink(const PolyView<double> &c, const double *p, double x0, double y0, double sw, double r_, double *a,
-                    int ast, Out &ro)
+    SDOT_HDI Sink(const P &c, const double *p, double x0, double y0, double sw, double r_, double *a, int ast,
+                  Out &ro)
         : cell(c), pos(p), c0x(x0), c0y(y0), sqw0(sw), cx(x0), cy(y0), r(r_), acc(a), acc_st(ast), row(ro) {}
 
     SDOT_HDI void begin_piece(double c) {
@@ -180,10 +181,11 @@ struct Sink {
 };
 
 // Records the ids of the streamed (disc-clipped) cell boundary.
+template <class P = PolyView<double>>
 struct NbSink {
-    const PolyView<double> &cell;
+    const P &cell;
     Out &out;
-    SDOT_HDI NbSink(const PolyView<double> &c, Out &o) : cell(c), out(o) {}
+    SDOT_HDI NbSink(const P &c, Out &o) : cell(c), out(o) {}
     SDOT_HDI void push(double, double, int tag) { out.emit(tag == ID_ARC ? ID_ARC : cell.I(tag), 0.0); }
     SDOT_HDI void finish() {}
 };
@@ -191,8 +193,8 @@ struct NbSink {
 // Streams a polygon; each vertex carries the index of the cell edge leaving
 // it: for the cell itself that is the vertex index, for a piece (a clipped
 // copy of the cell) it is the tag stored in its id slot.
-template <class Stage>
-SDOT_HDI void stream_cell(const PolyView<double> &cell, int n, Stage &st) {
+template <class Stage, class P>
+SDOT_HDI void stream_cell(const P &cell, int n, Stage &st) {
     for (int k = 0; k < n; ++k) st.push(cell.X(k), cell.Y(k), k);
     st.finish();
 }
@@ -259,16 +261,18 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             nd_a = nd.a;
             nd_b = nd.b;
         }
-        // ---- the vertex pass shared by both kinds of step
-        CutFacts f;
+        // ---- the vertex pass shared by both kinds of step (bit k: vertex k
+        // is outside the bisector, or fails the eviction test)
+        unsigned mask = 0;
         for (int k = 0; k < n; ++k) {
             const double px = cell.X(k), py = cell.Y(k);
             const double d = (ox - px) * nx + (oy - py) * ny;
             const double qx = fmin(hi0, fmax(lo0, px)), qy = fmin(hi1, fmax(lo1, py));
             const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
             const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - maxw;
-            f.add(k, n, is_cut ? d < 0.0 : !(lhs <= rhs));
+            mask |= unsigned(is_cut ? d < 0.0 : !(lhs <= rhs)) << k;
         }
+        const CutFacts f = cut_facts(mask, n);
         if (is_cut) {
             if (f.nb_out) {
                 n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
@@ -322,13 +326,293 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
     return n;
 }
 
+// ---------------------------------------------------------------- mixed FP32
+// FP32 build of the cell of Dirac s for the mixed-precision path, in
+// coordinates relative to c0 (vertex u = p - c0), so that the float error is
+// relative to the size of the cell rather than of the domain.  Same walk and
+// same steps as build_cell; the decisions are made safe this way:
+//  * a box is evicted only when every vertex passes the eviction test by more
+//    than the float rounding of its two sides (a wrong eviction could drop a
+//    neighbour; an extra visit only costs time);
+//  * a cut that classifies some vertex within the float rounding of the
+//    bisector stops the build with -3: the caller rebuilds the cell in FP64.
+// The polygon's edge ids then give the topology that the FP64 re-clip
+// (ReclipView) turns into exact vertices.  Returns like build_cell, or -3.
+constexpr float F32_MARGIN = 16.0f * 5.96e-8f;  // 16 float ulps, relative
+
+SDOT_KFN int build_cell_f32(const Cell2DArgs &A, long long s, const PolyView<float> &cell, int cap, double c0x,
+                            double c0y, double w0, bool local) {
+    const float w0f = float(w0);
+    int n = 0;
+    float span = 0;  // size of the starting polygon: the scale of the vertices' rounding
+    if (local) {
+        // Start from a local square of half-size R around c0 cut by the
+        // domain's edges, not from the domain itself: float vertices
+        // interpolated along domain-sized edges would carry errors at the
+        // domain's scale.  R is 3 times the farthest of the 12 Morton-order
+        // neighbours.  The square is exact for the cell when none of its
+        // edges survives (the eviction tests on the truncated polygon are
+        // then valid for the whole cell); otherwise the cell is rebuilt in
+        // FP64, or, when it only emptied within the square, walked again from
+        // the whole domain (-4).
+        double r2 = 0;
+        for (long long q = s - 6; q <= s + 6; ++q) {
+            if (q == s || q < 0 || q >= A.n) continue;
+            const double dx = A.pos[2 * q] - c0x, dy = A.pos[2 * q + 1] - c0y;
+            r2 = fmax(r2, dx * dx + dy * dy);
+        }
+        const float R = float(3.0 * sqrt(r2));
+        if (!(R > 0)) return -3;
+        span = 2 * R;
+        n = 4;
+        cell.X(0) = -R; cell.Y(0) = -R; cell.I(0) = ID_LOCAL;
+        cell.X(1) = R;  cell.Y(1) = -R; cell.I(1) = ID_LOCAL;
+        cell.X(2) = R;  cell.Y(2) = R;  cell.I(2) = ID_LOCAL;
+        cell.X(3) = -R; cell.Y(3) = R;  cell.I(3) = ID_LOCAL;
+        for (int e = 0; e < A.start_n && n > 0; ++e) {
+            const int e1 = e + 1 < A.start_n ? e + 1 : 0;
+            const double p0x = A.start_xy[2 * e] - c0x, p0y = A.start_xy[2 * e + 1] - c0y;
+            const double dx = A.start_xy[2 * e1] - A.start_xy[2 * e];
+            const double dy = A.start_xy[2 * e1 + 1] - A.start_xy[2 * e + 1];
+            n = plane_cut(cell, n, cap, float(p0x), float(p0y), float(dy), float(-dx), domain_id(e), true);
+        }
+        if (n <= 0) return -4;  // the square misses the domain
+    } else {
+        // the whole domain: used to decide cells that emptied within the
+        // square; a non-empty result goes to FP64
+        n = A.start_n;
+        for (int k = 0; k < n; ++k) {
+            cell.X(k) = float(A.start_xy[2 * k] - c0x);
+            cell.Y(k) = float(A.start_xy[2 * k + 1] - c0y);
+            cell.I(k) = domain_id(k);
+            span = fmaxf(span, fabsf(cell.X(k)) + fabsf(cell.Y(k)));
+        }
+        span *= 2;
+    }
+    auto has_local = [&]() {
+        for (int k = 0; k < n; ++k)
+            if (cell.I(k) == ID_LOCAL) return true;
+        return false;
+    };
+    int stack[STACK];
+    int sp = 0;
+    stack[sp++] = 0;
+    int j = 0, je = 0;
+    int visits = 0;
+    while (true) {
+        const bool is_cut = j < je;
+        float ox = 0, oy = 0, nx = 0, ny = 0;
+        float lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0, maxw = 0;
+        int node = -1, nd_a = 0, nd_b = 0;
+        if (is_cut) {
+            if (j == s) {
+                ++j;
+                continue;
+            }
+            (void)SDOT_CHECK_IDX(j, A.n, 6);
+            const double vx = A.pos[2 * j] - c0x, vy = A.pos[2 * j + 1] - c0y;
+            const double x = 0.5 + 0.5 * (w0 - A.w[j]) / (vx * vx + vy * vy);
+            nx = float(vx);
+            ny = float(vy);
+            ox = float(x * vx);
+            oy = float(x * vy);
+        } else {
+            if (sp == 0) break;
+            if (++visits > A.max_nodes) {
+                flag_error(A.err, DE_ITER);
+                return -1;
+            }
+            node = stack[--sp];
+            const TreeNode<2> &nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
+            lo0 = float(nd.lo[0] - c0x);
+            lo1 = float(nd.lo[1] - c0y);
+            hi0 = float(nd.hi[0] - c0x);
+            hi1 = float(nd.hi[1] - c0y);
+            maxw = float(nd.maxw);
+            nd_a = nd.a;
+            nd_b = nd.b;
+        }
+        unsigned mask = 0;
+        bool near = false;
+        for (int k = 0; k < n; ++k) {
+            const float px = cell.X(k), py = cell.Y(k);
+            const float ex = ox - px, ey = oy - py;
+            const float d = ex * nx + ey * ny;
+            const float qx = fminf(hi0, fmaxf(lo0, px)) - px, qy = fminf(hi1, fmaxf(lo1, py)) - py;
+            const float uu = px * px + py * py, qq = qx * qx + qy * qy;
+            const float lhs = uu - w0f, rhs = qq - maxw;
+            const float emargin = F32_MARGIN * (uu + fabsf(w0f) + qq + fabsf(maxw));
+            const bool o = is_cut ? d < 0.0f : !(lhs <= rhs - emargin);
+            // rounding of d: the products, the bisector's origin, and the
+            // vertex, whose error scales with the edges it was cut from
+            near |= is_cut && fabsf(d) <= F32_MARGIN * (fabsf(ex * nx) + fabsf(ey * ny) +
+                                                        (fabsf(ox) + fabsf(px) + span) * fabsf(nx) +
+                                                        (fabsf(oy) + fabsf(py) + span) * fabsf(ny));
+            mask |= unsigned(o) << k;
+        }
+        if (near) return -3;
+        const CutFacts f = cut_facts(mask, n);
+        if (is_cut) {
+            if (f.nb_out) {
+                if (f.nb_out == n && has_local()) return -4;  // empty within the square only
+                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
+                if (n <= 0) return n;
+            }
+            ++j;
+            continue;
+        }
+        if (f.nb_out == 0) continue;
+        if (nd_b < 0) {
+            const int first = nd_a, nch = -nd_b;
+            if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
+                guard_fail(A, 1, s, node);
+                return -2;
+            }
+            if (sp + nch > STACK) {
+                flag_error(A.err, DE_STACK);
+                return -1;
+            }
+            float key[4];
+            int ch[4];
+            for (int c = 0; c < nch; ++c) {
+                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
+                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
+                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
+                key[c] = float(mx * mx + my * my);
+                ch[c] = first + c;
+            }
+            for (int i = 1; i < nch; ++i) {
+                const float kk = key[i];
+                const int cc = ch[i];
+                int q = i - 1;
+                while (q >= 0 && key[q] < kk) {
+                    key[q + 1] = key[q];
+                    ch[q + 1] = ch[q];
+                    --q;
+                }
+                key[q + 1] = kk;
+                ch[q + 1] = cc;
+            }
+            for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
+        } else {
+            if (nd_a < 0 || nd_b > A.n) {
+                guard_fail(A, 2, s, node);
+                return -2;
+            }
+            j = nd_a;
+            je = nd_b;
+        }
+    }
+    return has_local() ? -3 : n;
+}
+
+// The FP64 polygon of a cell whose topology came from the FP32 build: vertex
+// k is the intersection of the lines of edges k - 1 and k (a weighted
+// bisector, or an edge of the starting polygon), solved in FP64 in
+// coordinates relative to c0 and shifted back.  X, Y, I as PolyView's.
+struct ReclipView {
+    const Cell2DArgs &A;
+    PolyView<float> poly;
+    int n;
+    double c0x, c0y, w0;
+    mutable int ck = -1;
+    mutable double vx = 0, vy = 0;
+
+    SDOT_HDI int I(int k) const { return poly.I(k); }
+    // line a . u = b of the edge with this id (u relative to c0)
+    SDOT_HDI void line(int id, double &ax, double &ay, double &b) const {
+        if (id >= 0) {
+            const double dx = A.pos[2 * id] - c0x, dy = A.pos[2 * id + 1] - c0y;
+            ax = dx;
+            ay = dy;
+            b = 0.5 * (dx * dx + dy * dy) + 0.5 * (w0 - A.w[id]);
+        } else {
+            const int e = domain_edge(id), e1 = e + 1 < A.start_n ? e + 1 : 0;
+            const double p0x = A.start_xy[2 * e] - c0x, p0y = A.start_xy[2 * e + 1] - c0y;
+            const double p1x = A.start_xy[2 * e1] - c0x, p1y = A.start_xy[2 * e1 + 1] - c0y;
+            ax = p0y - p1y;
+            ay = p1x - p0x;
+            b = ax * p0x + ay * p0y;
+        }
+    }
+    // intersection of edges k - 1 and k; returns |sin| of their angle
+    SDOT_HDI double solve(int k, double &ux, double &uy) const {
+        double a1x, a1y, b1, a2x, a2y, b2;
+        line(I(k == 0 ? n - 1 : k - 1), a1x, a1y, b1);
+        line(I(k), a2x, a2y, b2);
+        const double det = a1x * a2y - a1y * a2x;
+        ux = (b1 * a2y - b2 * a1y) / det;
+        uy = (a1x * b2 - a2x * b1) / det;
+        return fabs(det) / (sqrt(a1x * a1x + a1y * a1y) * sqrt(a2x * a2x + a2y * a2y));
+    }
+    SDOT_HDI void vert(int k) const {
+        if (k == ck) return;
+        double ux, uy;
+        solve(k, ux, uy);
+        vx = c0x + ux;
+        vy = c0y + uy;
+        ck = k;
+    }
+    SDOT_HDI double X(int k) const {
+        vert(k);
+        return vx;
+    }
+    SDOT_HDI double Y(int k) const {
+        vert(k);
+        return vy;
+    }
+    // The FP32 topology is the FP64 one when: every FP64 vertex is near its
+    // FP32 vertex, no two consecutive edges are nearly parallel, and every
+    // FP64 edge runs the way its FP32 edge does and is not nearly of zero
+    // length (a reversed or vanishing edge marks a vertex where four cells
+    // nearly meet, whose topology depends on rounding).
+    SDOT_HDI bool consistent() const {
+        double vx0 = 0, vy0 = 0, px = 0, py = 0, scale = 0;
+        float fx0 = 0, fy0 = 0, gx = 0, gy = 0;
+        for (int k = 0; k <= n && n >= 2; ++k) {
+            const int kk = k == n ? 0 : k;
+            double ux, uy;
+            if (k == n) {
+                ux = vx0;
+                uy = vy0;
+            } else {
+                const double sn = solve(kk, ux, uy);
+                if (!(sn > 1e-6)) return false;
+            }
+            const float fx = poly.X(kk), fy = poly.Y(kk);
+            const double sc = fabs(double(fx)) + fabs(double(fy)) + 1e-300;
+            if (!(fabs(ux - fx) + fabs(uy - fy) <= 1e-4 * sc)) return false;
+            scale = fmax(scale, sc);
+            if (k == 0) {
+                vx0 = ux;
+                vy0 = uy;
+                fx0 = fx;
+                fy0 = fy;
+            } else {
+                const double ex = ux - px, ey = uy - py;
+                const double fex = double(fx) - gx, fey = double(fy) - gy;
+                if (!(ex * fex + ey * fey > 0)) return false;
+                if (fabs(ex) + fabs(ey) <= 1e-7 * (sc + fabs(px) + fabs(py))) return false;
+            }
+            px = ux;
+            py = uy;
+            gx = fx;
+            gy = fy;
+        }
+        (void)fx0;
+        (void)fy0;
+        (void)scale;
+        return true;
+    }
+};
+
 // Per-cell work once the polygon of Dirac s is built (n vertices; -1: a
 // capacity was exceeded, -2: a guard failed).  Returns false when a capacity
 // was exceeded (the cell is then rebuilt by the next tier, which rewrites
 // every output of it).
-template <int MODE, bool BALL>
-SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int n, int cap, double *acc,
-                            int acc_st, const PolyView<double> &piece, Out &row, Out &nbo) {
+template <int MODE, bool BALL, class P>
+SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n, int cap, double *acc, int acc_st,
+                          const PolyView<double> &piece, Out &row, Out &nbo) {
     const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
     if (n == -2) {
         // failed guard: report a NaN cell, not an overflow
@@ -342,7 +626,8 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<doubl
 
     const double r = BALL ? sqrt(w0) : -1.0;
     constexpr bool DIRECT = MODE == DM_SINGLE;
-    Sink<DIRECT> sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
+    using SinkT = Sink<DIRECT, P>;
+    SinkT sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
     sink.n_diracs = A.n;
 
     if (MODE == DM_SINGLE && !BALL) {
@@ -367,7 +652,7 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<doubl
         }
     } else if (MODE == DM_SINGLE) {
         sink.begin_piece(A.coeff);
-        DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
+        DiscClip<SinkT> dc(sink, c0x, c0y, r);
         stream_cell(cell, n, dc);
         sink.end_piece(dc.result_radius());
     } else {
@@ -396,18 +681,18 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<doubl
                         const double x0 = A.img_lo[0] + psx * double(ix), x1 = A.img_lo[0] + psx * double(ix + 1);
                         sink.begin_piece(A.img[(long long)iy * A.img_nx + ix]);
                         if (BALL) {
-                            DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
-                            AxisClip<DiscClip<Sink<DIRECT>>> c4(dc, 1, y1, -1.0, PID_OWN);
-                            AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>> c3(c4, 1, y0, 1.0, PID_OWN);
-                            AxisClip<AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>>> c2(c3, 0, x1, -1.0, PID_OWN);
-                            AxisClip<AxisClip<AxisClip<AxisClip<DiscClip<Sink<DIRECT>>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                            DiscClip<SinkT> dc(sink, c0x, c0y, r);
+                            AxisClip<DiscClip<SinkT>> c4(dc, 1, y1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<DiscClip<SinkT>>> c3(c4, 1, y0, 1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<DiscClip<SinkT>>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<AxisClip<DiscClip<SinkT>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
                             stream_cell(cell, n, c1);
                             sink.end_piece(dc.result_radius());
                         } else {
-                            AxisClip<Sink<DIRECT>> c4(sink, 1, y1, -1.0, PID_OWN);
-                            AxisClip<AxisClip<Sink<DIRECT>>> c3(c4, 1, y0, 1.0, PID_OWN);
-                            AxisClip<AxisClip<AxisClip<Sink<DIRECT>>>> c2(c3, 0, x1, -1.0, PID_OWN);
-                            AxisClip<AxisClip<AxisClip<AxisClip<Sink<DIRECT>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                            AxisClip<SinkT> c4(sink, 1, y1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<SinkT>> c3(c4, 1, y0, 1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<SinkT>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                            AxisClip<AxisClip<AxisClip<AxisClip<SinkT>>>> c1(c2, 0, x0, 1.0, PID_OWN);
                             stream_cell(cell, n, c1);
                             sink.end_piece(-1.0);
                         }
@@ -431,7 +716,7 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<doubl
                     if (np < 0) return false;
                     sink.begin_piece(A.item_coeff[it]);
                     if (BALL) {
-                        DiscClip<Sink<DIRECT>> dc(sink, c0x, c0y, r);
+                        DiscClip<SinkT> dc(sink, c0x, c0y, r);
                         stream_piece(piece, np, dc);
                         sink.end_piece(dc.result_radius());
                     } else {
@@ -467,8 +752,8 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const PolyView<doubl
     }
     if (A.nb.cnt) {
         if (BALL) {
-            NbSink nbs(cell, nbo);
-            DiscClip<NbSink> dc(nbs, c0x, c0y, r);
+            NbSink<P> nbs(cell, nbo);
+            DiscClip<NbSink<P>> dc(nbs, c0x, c0y, r);
             stream_cell(cell, n, dc);
         } else {
             for (int k = 0; k < n; ++k) nbo.emit(cell.I(k), 0.0);
@@ -514,6 +799,49 @@ __global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
         if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
         if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
     } else {
+        const int k = atomicAdd(A.ovf_cnt, 1);
+        A.ovf_list[k] = int(s);
+    }
+}
+
+// Fast tier of the mixed-precision path: FP32 build (polygon as floats in
+// shared memory), FP64 re-clip of its vertices and FP64 integration.  Cells
+// whose FP32 decisions were too close to call, whose topology does not
+// re-clip cleanly, or that overflow the capacity go to the FP64 warp tier.
+template <int MODE, bool BALL>
+__global__ void __launch_bounds__(T2D) k_cells2d_mixed(const Cell2DArgs A) {
+    extern __shared__ double smem[];
+    constexpr int CAP = CAP_FAST_2D;
+    const int t = threadIdx.x;
+    float *sx = reinterpret_cast<float *>(smem);
+    float *sy = sx + CAP * T2D;
+    int *sid = reinterpret_cast<int *>(sy + CAP * T2D);
+    double *extra = reinterpret_cast<double *>(sid + CAP * T2D);
+    PolyView<float> cell{sx + t, sy + t, sid + t, T2D, CAP};
+    double *acc = extra + t;
+    const PolyView<double> no_piece{nullptr, nullptr, nullptr, T2D, 0};  // several shapes never take this path
+    const long long s = blockIdx.x * (long long)T2D + t;
+    if (s >= A.n) return;
+    const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
+    int n = build_cell_f32(A, s, cell, CAP, c0x, c0y, w0, true);
+    if (n == -4) {
+        n = build_cell_f32(A, s, cell, CAP, c0x, c0y, w0, false);
+        if (n > 0) n = -3;  // only an empty cell is decided by the domain-wide FP32 walk
+    }
+    const ReclipView view{A, cell, n > 0 ? n : 0, c0x, c0y, w0};
+    bool ok = n >= 0 || n == -2;
+    if (n > 0 && !view.consistent()) ok = false;
+    if (ok) {
+        Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride,
+                A.rows.cap);
+        Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
+        ok = finish_cell<MODE, BALL>(A, s, view, n, CAP, acc, T2D, no_piece, row, nbo);
+        if (ok) {
+            if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
+            if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
+        }
+    }
+    if (!ok) {
         const int k = atomicAdd(A.ovf_cnt, 1);
         A.ovf_list[k] = int(s);
     }
@@ -705,7 +1033,12 @@ void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
         SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         attr_set = true;
     }
-    k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
+    if (MODE != DM_MULTI && a.mixed) {
+        const size_t smem_m = size_t(CAP) * T2D * 12 + size_t(smem_extra_halves<MODE>()) * CAP * T2D * 4;
+        k_cells2d_mixed<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem_m, st>>>(a);
+    } else {
+        k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
+    }
     note_launch();
     SDOT_CUDA(cudaGetLastError());
     k_cells2d_wtier<MODE, BALL><<<WTIER_WARPS / 4, 128, 0, st>>>(a, static_cast<double *>(scratch), WTIER_WARPS,

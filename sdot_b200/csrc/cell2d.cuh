@@ -13,6 +13,7 @@ enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2 };
 // global scratch).  Beyond the warp tier's capacity the call reports
 // ST_CAPACITY.
 constexpr int CAP_FAST_2D = 16;
+static_assert(CAP_FAST_2D <= 32, "the fast tier keeps one bit per vertex in a 32-bit mask");
 constexpr int CAP_HUGE_2D = 1024;
 // Hessian rows and neighbour lists are stored slot-major (ELL) with these
 // widths; longer rows (only cells of the warp tier) go to a side buffer,
@@ -51,6 +52,7 @@ struct Cell2DArgs {
     const double *start_xy = nullptr;  // 2 * start_n
     double coeff = 1.0;                // single-item density
     int mode = DM_SINGLE;
+    int mixed = 0;                     // FP32 build + FP64 re-clip (SDOT_MIXED)
     int ball = 0;
     // image (nb_coeffs == 1)
     double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};

@@ -1,0 +1,587 @@
+// 3D Laguerre-cell kernels (see cell3d.cuh).
+//
+// One warp builds one cell.  The cell is a convex polyhedron held as its
+// faces, one face per lane (two in the large pass): each face is a polygon
+// (vertices counter-clockwise seen from outside, in coordinates relative to
+// the cell's Dirac) whose edge k carries the id of the face across it, plus
+// the face's plane a . u <= b and its cut id (a Dirac index, or a domain
+// face).  A plane cut is then a 2D polygon cut done by every lane on its own
+// face at once, followed by the new face, whose vertices are the points where
+// the cut faces enter the cut: starting from one cut face, the next is the
+// face across its exit edge.  The point where an edge is cut is computed from
+// the edge's inside vertex in both faces that share the edge, so the copies
+// agree bitwise and the new face closes exactly.
+//
+// Reference behaviour restated (ConvexPolyhedron3 and the 3D traversal):
+//  * traversal and eviction test: SpZGrid::for_each_laguerre_cell, as in 2D
+//    (SpZGrid.tcc:494-719, eviction :475-480), weighted bisector :506-522;
+//  * volume: sum over faces of (O . N) area / 3 (ConvexPolyhedron3.tcc:1022-1057),
+//    here with the cell's Dirac as the apex (O . N is the signed distance of the
+//    face plane from it);
+//  * centroid: pyramid centroids weighted by their volumes
+//    (ConvexPolyhedron3::add_centroid_contrib, ConvexPolyhedron3.tcc:884-924);
+//  * face area by a fan of triangles (ConvexPolyhedron3::area, :1367-1419);
+//  * Hessian row: -1/2 coeff area / |x_i - x_j| per neighbour face, the
+//    diagonal their sum; domain faces skipped (get_der_integrals_wrt_weights.h:43-88).
+#include "cell3d.cuh"
+
+namespace sdot {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int STACK3 = 96;  // depth <= 10 levels (10 key bits per axis), <= 7 pending siblings each
+
+// Faces of one warp: vertex v of face slot f at [v * MAXF + f].
+template <int FPL, int MAXV>
+struct Faces {
+    static constexpr int MAXF = 32 * FPL;
+    double *X, *Y, *Z;
+    int *E;
+    __device__ int at(int v, int f) const { return v * MAXF + f; }
+};
+
+template <int FPL, int MAXV>
+constexpr size_t warp_smem_bytes() {
+    return size_t(MAXV) * (32 * FPL) * (3 * sizeof(double) + sizeof(int)) + STACK3 * sizeof(int);
+}
+
+// One cell's state in a warp: the faces (shared memory) and, per lane and
+// face slot r (face lane + 32 r), the face's plane, id and vertex count.
+template <int FPL, int MAXV>
+struct Cell3 {
+    Faces<FPL, MAXV> F;
+    int *stack;
+    int fid[FPL], nv[FPL];
+    double ax[FPL], ay[FPL], az[FPL], b[FPL];
+};
+
+__device__ inline double shfl(double v, int src) { return __shfl_sync(FULL, v, src); }
+
+// Outcome of a cut: 0 done, 1 a capacity was exceeded, 2 degenerate geometry.
+template <int FPL, int MAXV>
+__device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double qb, int qid) {
+    const int lane = threadIdx.x & 31;
+    auto &F = C.F;
+    unsigned mask[FPL];
+    bool has = false;
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        unsigned m = 0;
+        for (int v = 0; v < C.nv[r]; ++v) {
+            const int i = F.at(v, f);
+            const double d = qb - (qx * F.X[i] + qy * F.Y[i] + qz * F.Z[i]);
+            m |= unsigned(d < 0.0) << v;
+        }
+        mask[r] = m;
+        has |= m != 0;
+    }
+    if (!__any_sync(FULL, has)) return 0;
+    // ---- cut every face
+    bool cut[FPL];
+    int exit_nb[FPL];
+    double ex[FPL], ey[FPL], ez[FPL];  // entry point of each cut face
+    bool bad = false, over = false;
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        cut[r] = false;
+        exit_nb[r] = 0;
+        ex[r] = ey[r] = ez[r] = 0;
+        const int n = C.nv[r];
+        if (n == 0 || mask[r] == 0) continue;
+        const unsigned full = n >= 32 ? FULL : ((1u << n) - 1u);
+        const unsigned outs = mask[r] & full;
+        if (outs == full) {  // the whole face is removed
+            C.nv[r] = 0;
+            continue;
+        }
+        // out vertex k whose predecessor is in: the start of the outside run
+        const unsigned prev_out = ((outs << 1) | (outs >> (n - 1))) & full;  // bit k: vertex k - 1 is out
+        const unsigned starts = outs & ~prev_out;
+        const unsigned next_out = ((outs >> 1) | (outs << (n - 1))) & full;  // bit k: vertex k + 1 is out
+        const unsigned ends = outs & ~next_out;
+        if (__popc(starts) != 1 || __popc(ends) != 1) {
+            bad = true;
+            continue;
+        }
+        const int o1 = __ffs(starts) - 1, o2 = __ffs(ends) - 1;
+        const int nout = __popc(outs);
+        const int il = o1 == 0 ? n - 1 : o1 - 1;  // last inside vertex before the run
+        const int fi = o2 == n - 1 ? 0 : o2 + 1;  // first inside vertex after it
+        const int nn = n - nout + 2;
+        if (nn > MAXV) {
+            over = true;
+            continue;
+        }
+        // the two new points, each from its edge's inside vertex
+        auto interp = [&](int vin, int vout, double &px, double &py, double &pz) {
+            const int a = F.at(vin, f), c = F.at(vout, f);
+            const double din = qb - (qx * F.X[a] + qy * F.Y[a] + qz * F.Z[a]);
+            const double dout = qb - (qx * F.X[c] + qy * F.Y[c] + qz * F.Z[c]);
+            const double t = din / (din - dout);
+            px = F.X[a] + t * (F.X[c] - F.X[a]);
+            py = F.Y[a] + t * (F.Y[c] - F.Y[a]);
+            pz = F.Z[a] + t * (F.Z[c] - F.Z[a]);
+        };
+        double xx, xy, xz, nx, ny, nz;
+        interp(il, o1, xx, xy, xz);  // exit point, on edge il -> o1
+        interp(fi, o2, nx, ny, nz);  // entry point, on edge o2 -> fi
+        const int xnb = F.E[F.at(il, f)], nnb = F.E[F.at(o2, f)];
+        auto move = [&](int dst, int src) {
+            const int a = F.at(dst, f), c = F.at(src, f);
+            F.X[a] = F.X[c];
+            F.Y[a] = F.Y[c];
+            F.Z[a] = F.Z[c];
+            F.E[a] = F.E[c];
+        };
+        int px_at;  // index of the exit point in the new polygon
+        if (o1 <= o2) {
+            // outside run inside the list: [0, o1) X N [o2 + 1, n)
+            const int delta = (o1 + 2) - (o2 + 1);
+            if (delta > 0)
+                for (int k = n - 1; k > o2; --k) move(k + delta, k);
+            else if (delta < 0)
+                for (int k = o2 + 1; k < n; ++k) move(k + delta, k);
+            px_at = o1;
+        } else {
+            // the outside run wraps: inside run [o2 + 1, o1) moves to the front
+            const int m = o1 - o2 - 1;
+            for (int k = 0; k < m; ++k) move(k, o2 + 1 + k);
+            px_at = m;
+        }
+        const int a0 = F.at(px_at, f), a1 = F.at(px_at + 1, f);
+        F.X[a0] = xx;
+        F.Y[a0] = xy;
+        F.Z[a0] = xz;
+        F.E[a0] = qid;
+        F.X[a1] = nx;
+        F.Y[a1] = ny;
+        F.Z[a1] = nz;
+        F.E[a1] = nnb;
+        C.nv[r] = nn;
+        cut[r] = true;
+        exit_nb[r] = xnb;
+        ex[r] = nx;
+        ey[r] = ny;
+        ez[r] = nz;
+    }
+    if (__any_sync(FULL, bad)) return 2;
+    if (__any_sync(FULL, over)) return 1;
+    // ---- the new face: a free slot, vertices chained over the cut faces
+    unsigned cutm[FPL], freem[FPL];
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        cutm[r] = __ballot_sync(FULL, cut[r]);
+        freem[r] = __ballot_sync(FULL, C.nv[r] == 0);
+    }
+    int m = 0, slot = -1, start = -1;
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        m += __popc(cutm[r]);
+        if (slot < 0 && freem[r]) slot = 32 * r + __ffs(freem[r]) - 1;
+        if (start < 0 && cutm[r]) start = 32 * r + __ffs(cutm[r]) - 1;
+    }
+    if (m == 0) return 0;  // only whole faces were removed
+    if (m < 3) return 2;
+    if (slot < 0 || m > MAXV) return 1;
+    int cur = start;
+    for (int i = 0; i < m; ++i) {
+        // broadcast the current cut face's entry point, exit neighbour and id
+        const int cl = cur & 31, cr = cur >> 5;
+        double px = 0, py = 0, pz = 0;
+        int nb = 0, id = 0;
+#pragma unroll
+        for (int r = 0; r < FPL; ++r)
+            if (r == cr) {
+                px = shfl(ex[r], cl);
+                py = shfl(ey[r], cl);
+                pz = shfl(ez[r], cl);
+                nb = __shfl_sync(FULL, exit_nb[r], cl);
+                id = __shfl_sync(FULL, C.fid[r], cl);
+            }
+        if (lane == (slot & 31)) {
+            const int a = F.at(i, slot);
+            F.X[a] = px;
+            F.Y[a] = py;
+            F.Z[a] = pz;
+            F.E[a] = id;
+        }
+        // next: the cut face whose id is the exit neighbour
+        int next = -1;
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) {
+            const unsigned hit = __ballot_sync(FULL, cut[r] && C.fid[r] == nb);
+            if (next < 0 && hit) next = 32 * r + __ffs(hit) - 1;
+        }
+        if (next < 0) return 2;
+        cur = next;
+    }
+    if (cur != start) return 2;
+#pragma unroll
+    for (int r = 0; r < FPL; ++r)
+        if (lane + 32 * r == slot) {
+            C.fid[r] = qid;
+            C.nv[r] = m;
+            C.ax[r] = qx;
+            C.ay[r] = qy;
+            C.az[r] = qz;
+            C.b[r] = qb;
+        }
+    __syncwarp();
+    return 0;
+}
+
+// The domain box as six faces (slots 0..5), relative to c0.
+template <int FPL, int MAXV>
+__device__ void init_box(Cell3<FPL, MAXV> &C, const Cell3DArgs &A, double c0x, double c0y, double c0z) {
+    const int lane = threadIdx.x & 31;
+    const double lo[3] = {A.box_lo[0] - c0x, A.box_lo[1] - c0y, A.box_lo[2] - c0z};
+    const double hi[3] = {A.box_hi[0] - c0x, A.box_hi[1] - c0y, A.box_hi[2] - c0z};
+    // corners: bit 0 -> x, bit 1 -> y, bit 2 -> z (0: lo, 1: hi)
+    // per face: 4 corners counter-clockwise seen from outside, and the face
+    // across each edge (faces: 0 x-lo, 1 x-hi, 2 y-lo, 3 y-hi, 4 z-lo, 5 z-hi)
+    constexpr int corner[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
+    constexpr int across[6][4] = {{2, 5, 3, 4}, {4, 3, 5, 2}, {4, 1, 5, 0}, {0, 5, 1, 4}, {0, 3, 1, 2}, {2, 1, 3, 0}};
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        C.nv[r] = 0;
+        C.fid[r] = 0;
+        C.ax[r] = C.ay[r] = C.az[r] = C.b[r] = 0;
+        if (f < 6) {
+            const int ax = f >> 1, side = f & 1;
+            C.nv[r] = 4;
+            C.fid[r] = domain_id(f);
+            double nrm[3] = {0, 0, 0};
+            nrm[ax] = side ? 1.0 : -1.0;
+            C.ax[r] = nrm[0];
+            C.ay[r] = nrm[1];
+            C.az[r] = nrm[2];
+            C.b[r] = side ? hi[ax] : -lo[ax];
+            for (int v = 0; v < 4; ++v) {
+                const int c = corner[f][v];
+                const int a = C.F.at(v, f);
+                C.F.X[a] = (c & 1) ? hi[0] : lo[0];
+                C.F.Y[a] = (c & 2) ? hi[1] : lo[1];
+                C.F.Z[a] = (c & 4) ? hi[2] : lo[2];
+                C.F.E[a] = domain_id(across[f][v]);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Writes a row of `cnt` entries: the lanes' neighbour faces (slot r of a
+// lane writes entry pos[r] when mine[r]), then the diagonal from lane 0 when
+// with_diag, into the ELL slots or, for a long row, the side buffer.
+template <int FPL>
+__device__ bool write_row(const Rows &R, long long s, int cnt, const int *pos, const bool *mine, const int *col,
+                          const double *val, bool with_diag, int diag_col, double diag_val) {
+    const int lane = threadIdx.x & 31;
+    long long off = 0;
+    const bool side = cnt > R.cap;
+    if (side) {
+        unsigned long long o = 0;
+        if (lane == 0) o = atomicAdd(R.side_used, (unsigned long long)cnt);
+        o = __shfl_sync(FULL, o, 0);
+        if ((long long)(o + cnt) > R.side_cap) return false;
+        off = (long long)o;
+        if (lane == 0) R.side[s] = off;
+    }
+    auto put = [&](int k, int c, double v) {
+        if (side) {
+            R.side_col[off + k] = c;
+            if (R.side_val) R.side_val[off + k] = v;
+        } else {
+            R.col[k * R.stride + s] = c;
+            if (R.val) R.val[k * R.stride + s] = v;
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < FPL; ++r)
+        if (mine[r]) put(pos[r], col[r], val[r]);
+    if (with_diag && lane == 0) put(cnt - 1, diag_col, diag_val);
+    if (lane == 0) R.cnt[s] = cnt;
+    return true;
+}
+
+// First failed guard of a 3D cell (the 2D kernels' guard_fail).
+__device__ void guard_fail3(const Cell3DArgs &A, int code, long long s, long long value) {
+    if (A.guard && atomicCAS(&A.guard[0], 0, code) == 0) {
+        A.guard[1] = int(s);
+        A.guard[2] = int(value);
+    }
+    flag_error(A.err, DE_GUARD);
+}
+
+// Builds and integrates the cell of sorted Dirac s.  Returns 0 (outputs
+// written), 1 (a capacity was exceeded: retry in the large pass), 2 (failed:
+// outputs written as NaN / empty row, error flagged).
+template <int FPL, int MAXV>
+__device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
+    const int lane = threadIdx.x & 31;
+    const double c0x = A.pos[3 * s], c0y = A.pos[3 * s + 1], c0z = A.pos[3 * s + 2], w0 = A.w[s];
+    init_box(C, A, c0x, c0y, c0z);
+    int status = 0;
+    if (lane == 0) C.stack[0] = 0;
+    __syncwarp();
+    int sp = 1;
+    for (int visits = 0; sp > 0 && status == 0; ++visits) {
+        if (visits > A.max_nodes) {
+            if (lane == 0) flag_error(A.err, DE_ITER);
+            status = 2;
+            break;
+        }
+        const int node = C.stack[--sp];
+        __syncwarp();
+        const TreeNode<3> nd = A.nodes[node];
+        // eviction test (SpZGrid.tcc:475-480) on every vertex of every face
+        const double lo0 = nd.lo[0] - c0x, lo1 = nd.lo[1] - c0y, lo2 = nd.lo[2] - c0z;
+        const double hi0 = nd.hi[0] - c0x, hi1 = nd.hi[1] - c0y, hi2 = nd.hi[2] - c0z;
+        bool fail = false;
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) {
+            const int f = lane + 32 * r;
+            for (int v = 0; v < C.nv[r] && !fail; ++v) {
+                const int i = C.F.at(v, f);
+                const double px = C.F.X[i], py = C.F.Y[i], pz = C.F.Z[i];
+                const double qx = fmin(hi0, fmax(lo0, px)) - px, qy = fmin(hi1, fmax(lo1, py)) - py,
+                             qz = fmin(hi2, fmax(lo2, pz)) - pz;
+                const double lhs = px * px + py * py + pz * pz - w0;
+                const double rhs = qx * qx + qy * qy + qz * qz - nd.maxw;
+                fail = !(lhs <= rhs);
+            }
+        }
+        if (!__any_sync(FULL, fail)) continue;
+        if (nd.b < 0) {
+            const int first = nd.a, nch = -nd.b;
+            if (nch < 2 || nch > 8 || first < 1 || first + nch > A.max_nodes) {
+                if (lane == 0) guard_fail3(A, 1, s, node);
+                status = 2;
+                break;
+            }
+            if (sp + nch > STACK3) {
+                if (lane == 0) flag_error(A.err, DE_STACK);
+                status = 2;
+                break;
+            }
+            // children sorted farthest first (nearest popped first); lane c
+            // keys child c, lane 0 sorts and pushes
+            float key = 0;
+            if (lane < nch) {
+                const TreeNode<3> &cn = A.nodes[first + lane];
+                const double mx = 0.5 * (cn.lo[0] + cn.hi[0]) - c0x, my = 0.5 * (cn.lo[1] + cn.hi[1]) - c0y,
+                             mz = 0.5 * (cn.lo[2] + cn.hi[2]) - c0z;
+                key = float(mx * mx + my * my + mz * mz);
+            }
+            float keys[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) keys[c] = __shfl_sync(FULL, key, c);
+            if (lane == 0) {
+                int ch[8];
+                for (int c = 0; c < nch; ++c) ch[c] = first + c;
+                for (int i = 1; i < nch; ++i) {
+                    const float kk = keys[i];
+                    const int cc = ch[i];
+                    int q = i - 1;
+                    while (q >= 0 && keys[q] < kk) {
+                        keys[q + 1] = keys[q];
+                        ch[q + 1] = ch[q];
+                        --q;
+                    }
+                    keys[q + 1] = kk;
+                    ch[q + 1] = cc;
+                }
+                for (int c = 0; c < nch; ++c) C.stack[sp + c] = ch[c];
+            }
+            __syncwarp();
+            sp += nch;
+        } else {
+            if (nd.a < 0 || nd.b > A.n) {
+                if (lane == 0) guard_fail3(A, 2, s, node);
+                status = 2;
+                break;
+            }
+            for (int j = nd.a; j < nd.b && status == 0; ++j) {
+                if (j == s) continue;
+                // weighted bisector, relative to c0: V . u <= 1/2 |V|^2 + 1/2 (w0 - w1)
+                const double vx = A.pos[3 * j] - c0x, vy = A.pos[3 * j + 1] - c0y, vz = A.pos[3 * j + 2] - c0z;
+                const double qb = 0.5 * (vx * vx + vy * vy + vz * vz) + 0.5 * (w0 - A.w[j]);
+                const int r = cut3(C, vx, vy, vz, qb, j);
+                if (r) status = r;
+            }
+        }
+    }
+    if (status == 1) return 1;
+    // ---- integrals over the faces (pyramids with apex c0)
+    double vol = 0, mx = 0, my = 0, mz = 0, der0 = 0;
+    int nrow = 0, nnb = 0;
+    int rpos[FPL], npos[FPL];
+    double rval[FPL];
+    bool rmine[FPL], nmine[FPL];
+    if (status == 0) {
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) {
+            const int f = lane + 32 * r;
+            const int n = C.nv[r];
+            rmine[r] = false;
+            nmine[r] = n > 0;
+            rval[r] = 0;
+            if (n < 3) continue;
+            const double na = sqrt(C.ax[r] * C.ax[r] + C.ay[r] * C.ay[r] + C.az[r] * C.az[r]);
+            const double ux = C.ax[r] / na, uy = C.ay[r] / na, uz = C.az[r] / na;
+            const int i0 = C.F.at(0, f);
+            const double x0 = C.F.X[i0], y0 = C.F.Y[i0], z0 = C.F.Z[i0];
+            double area = 0, fx = 0, fy = 0, fz = 0;
+            for (int k = 1; k + 1 < n; ++k) {
+                const int i1 = C.F.at(k, f), i2 = C.F.at(k + 1, f);
+                const double e1x = C.F.X[i1] - x0, e1y = C.F.Y[i1] - y0, e1z = C.F.Z[i1] - z0;
+                const double e2x = C.F.X[i2] - x0, e2y = C.F.Y[i2] - y0, e2z = C.F.Z[i2] - z0;
+                const double ta = 0.5 * ((e1y * e2z - e1z * e2y) * ux + (e1z * e2x - e1x * e2z) * uy +
+                                         (e1x * e2y - e1y * e2x) * uz);
+                area += ta;
+                fx += ta * (3 * x0 + e1x + e2x);
+                fy += ta * (3 * y0 + e1y + e2y);
+                fz += ta * (3 * z0 + e1z + e2z);
+            }
+            const double h = C.b[r] / na;  // signed distance of the face plane from c0
+            const double v = h * area / 3;
+            vol += v;
+            // pyramid centroid: 3/4 of the way from the apex to the face centroid
+            if (area != 0) {
+                const double k = v * 0.75 / (3 * area);
+                mx += k * fx;
+                my += k * fy;
+                mz += k * fz;
+            }
+            if (C.fid[r] >= 0) {
+                const double bd = 0.5 * A.coeff * area / na;  // |x_i - x_j| = |a|
+                rmine[r] = true;
+                rval[r] = -bd;
+                der0 += bd;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            vol += __shfl_xor_sync(FULL, vol, o);
+            mx += __shfl_xor_sync(FULL, mx, o);
+            my += __shfl_xor_sync(FULL, my, o);
+            mz += __shfl_xor_sync(FULL, mz, o);
+            der0 += __shfl_xor_sync(FULL, der0, o);
+        }
+        // positions of the row and neighbour entries: slot order
+        const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) {
+            const unsigned rm = __ballot_sync(FULL, rmine[r]), nm = __ballot_sync(FULL, nmine[r]);
+            rpos[r] = nrow + __popc(rm & below);
+            npos[r] = nnb + __popc(nm & below);
+            nrow += __popc(rm);
+            nnb += __popc(nm);
+        }
+    }
+    bool ok = true;
+    if (status == 0) {
+        const double mass = A.coeff * vol;
+        if (lane == 0) {
+            if (A.mass) A.mass[s] = mass;
+            if (A.ctd) {
+                const bool empty = vol == 0;
+                A.ctd[3 * s] = empty ? 0.0 : c0x + mx / vol;
+                A.ctd[3 * s + 1] = empty ? 0.0 : c0y + my / vol;
+                A.ctd[3 * s + 2] = empty ? 0.0 : c0z + mz / vol;
+            }
+        }
+        if (A.rows.cnt) ok &= write_row<FPL>(A.rows, s, nrow + 1, rpos, rmine, C.fid, rval, true, int(s), der0);
+        if (A.nb.cnt) ok &= write_row<FPL>(A.nb, s, nnb, npos, nmine, C.fid, rval, false, 0, 0.0);
+        ok = __all_sync(FULL, ok);
+    }
+    if (status == 2 || !ok) {
+        if (lane == 0) {
+            flag_error(A.err, status == 2 ? DE_DEGEN : DE_CAPACITY);
+            if (A.mass) A.mass[s] = nan("");
+            if (A.ctd) A.ctd[3 * s] = A.ctd[3 * s + 1] = A.ctd[3 * s + 2] = nan("");
+            if (A.rows.cnt) {
+                A.rows.cnt[s] = 1;
+                A.rows.col[s] = int(s);
+                A.rows.val[s] = 0.0;
+            }
+            if (A.nb.cnt) A.nb.cnt[s] = 0;
+        }
+        return 2;
+    }
+    return 0;
+}
+
+template <int FPL, int MAXV>
+__global__ void __launch_bounds__(64) k_cells3d(const Cell3DArgs A, const int *list, const int *list_cnt,
+                                                int *next_list, int *next_cnt, int nwarps) {
+    extern __shared__ double smem3[];
+    constexpr int MAXF = 32 * FPL;
+    constexpr size_t WB = warp_smem_bytes<FPL, MAXV>();
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+    char *base = reinterpret_cast<char *>(smem3) + WB * wib;
+    Cell3<FPL, MAXV> C;
+    C.F.X = reinterpret_cast<double *>(base);
+    C.F.Y = C.F.X + MAXV * MAXF;
+    C.F.Z = C.F.Y + MAXV * MAXF;
+    C.F.E = reinterpret_cast<int *>(C.F.Z + MAXV * MAXF);
+    C.stack = C.F.E + MAXV * MAXF;
+    const long long cnt = list ? *list_cnt : A.n;
+    for (long long i = gw; i < cnt; i += nwarps) {
+        const long long s = list ? list[i] : i;
+        const int r = cell3d<FPL, MAXV>(A, s, C);
+        if (r == 1) {
+            if (next_list) {
+                if (lane == 0) next_list[atomicAdd(next_cnt, 1)] = int(s);
+            } else if (lane == 0) {
+                flag_error(A.err, DE_CAPACITY);
+                if (A.mass) A.mass[s] = nan("");
+                if (A.ctd) A.ctd[3 * s] = A.ctd[3 * s + 1] = A.ctd[3 * s + 2] = nan("");
+                if (A.rows.cnt) {
+                    A.rows.cnt[s] = 1;
+                    A.rows.col[s] = int(s);
+                    A.rows.val[s] = 0.0;
+                }
+                if (A.nb.cnt) A.nb.cnt[s] = 0;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int FPL, int MAXV, int WPB>
+void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *next_list, int *next_cnt, long long ncells,
+             cudaStream_t st) {
+    constexpr size_t smem = warp_smem_bytes<FPL, MAXV>() * WPB;
+    static bool attr = false;
+    if (!attr) {
+        SDOT_CUDA(cudaFuncSetAttribute(k_cells3d<FPL, MAXV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        attr = true;
+    }
+    const long long max_blocks = 148LL * (FPL == 1 ? 7 : 3);
+    long long blocks = (ncells + WPB - 1) / WPB;
+    if (blocks > max_blocks) blocks = max_blocks;
+    if (blocks < 1) blocks = 1;
+    k_cells3d<FPL, MAXV><<<int(blocks), 32 * WPB, smem, st>>>(a, list, list_cnt, next_list, next_cnt,
+                                                               int(blocks) * WPB);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void cells3d_launch(const Cell3DArgs &a, cudaStream_t st) {
+    if (a.n == 0) return;
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+    if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
+    if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
+    launch3<1, 16, 2>(a, nullptr, nullptr, a.ovf_list, a.ovf_cnt, a.n, st);
+    // the large pass takes the overflow list (its length is on the device:
+    // every resident warp of the launch checks it)
+    launch3<2, 32, 1>(a, a.ovf_list, a.ovf_cnt, nullptr, nullptr, 148LL * 3, st);
+}
+
+}  // namespace sdot

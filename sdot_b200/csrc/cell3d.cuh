@@ -1,0 +1,37 @@
+// 3D Laguerre-cell kernels (sm_100a), FP64: cell volumes, centroids, Hessian
+// rows (face area / |x_i - x_j|) and neighbour lists.
+#pragma once
+#include "cell2d.cuh"
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace sdot {
+
+// Hessian rows and neighbour lists of 3D cells (ELL widths; longer rows go to
+// the side buffer of Rows).
+constexpr int ROWCAP_3D = 32;
+constexpr int NBCAP_3D = 48;
+
+struct Cell3DArgs {
+    long long n = 0;
+    const double *pos = nullptr;  // 3n, sorted order
+    const double *w = nullptr;    // n, sorted order
+    const TreeNode<3> *nodes = nullptr;
+    int max_nodes = 1 << 30;
+    double box_lo[3] = {0, 0, 0}, box_hi[3] = {1, 1, 1};  // the domain (one box)
+    double coeff = 1.0;                                    // its density
+    double *mass = nullptr;  // n
+    double *ctd = nullptr;   // 3n
+    Rows rows;               // Hessian rows (rows.cnt null: skipped)
+    Rows nb;                 // neighbour ids (nb.cnt null: skipped)
+    int *ovf_list = nullptr;  // cells handed to the large-capacity pass
+    int *ovf_cnt = nullptr;
+    unsigned *err = nullptr;
+    int *guard = nullptr;
+};
+
+// First pass over every cell (up to 32 faces of 16 vertices), then the cells
+// that overflowed it (up to 64 faces of 32 vertices).
+void cells3d_launch(const Cell3DArgs &a, cudaStream_t st);
+
+}  // namespace sdot

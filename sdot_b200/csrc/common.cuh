@@ -28,6 +28,9 @@ constexpr int ID_ARC = -2;
 constexpr int ID_DOMAIN0 = -3;
 __host__ __device__ inline int domain_id(int e) { return ID_DOMAIN0 - e; }
 __host__ __device__ inline int domain_edge(int id) { return ID_DOMAIN0 - id; }
+// Edges of the local square that starts an FP32 build (mixed path); a cell
+// that keeps one is rebuilt in FP64, so these ids never reach an output.
+constexpr int ID_LOCAL = -(1 << 30);
 
 // Inside a piece (cell intersected with a domain item or a pixel):
 //  id >= 0       : came from edge `id` of the cell polygon
@@ -99,6 +102,7 @@ enum DevErr : unsigned {
     DE_ITER = 4u,          // an iteration cap was reached
     DE_PIECE = 8u,         // a piece overflowed its capacity
     DE_GUARD = 16u,        // an input failed a consistency guard (see the debug triple)
+    DE_DEGEN = 32u,        // a 3D cut met degenerate geometry (a face cut twice, an open new face)
 };
 
 }  // namespace sdot

@@ -63,6 +63,26 @@ struct CutFacts {
     }
 };
 
+// The same facts from a bit mask of the outside vertices (bit k: vertex k;
+// polygons of at most 32 vertices).
+SDOT_HD CutFacts cut_facts(unsigned mask, int n) {
+    CutFacts f;
+    const unsigned valid = n >= 32 ? 0xffffffffu : ((1u << n) - 1u);
+    const unsigned in = ~mask & valid;
+#ifdef __CUDA_ARCH__
+    f.nb_out = __popc(mask);
+    f.first_out = __ffs(int(mask)) - 1;
+    f.first_in = __ffs(int(in)) - 1;
+#else
+    f.nb_out = __builtin_popcount(mask);
+    f.first_out = __builtin_ffs(int(mask)) - 1;
+    f.first_in = __builtin_ffs(int(in)) - 1;
+#endif
+    f.out1 = n > 1 && ((mask >> 1) & 1u);
+    f.out_last = (mask >> (n - 1)) & 1u;
+    return f;
+}
+
 template <class T>
 SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize,
                             const CutFacts &f);

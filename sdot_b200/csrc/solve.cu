@@ -261,7 +261,7 @@ namespace {
 
 template <class M>
 PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                  int max_iter, const PcgWork &w, cudaStream_t st, int check) {
+                  int max_iter, const PcgWork &w, cudaStream_t st, int check, bool graph) {
     PcgResult res;
     if (n <= 0) {
         res.converged = true;
@@ -284,21 +284,44 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
         return res;
     }
     const double target = rel_tol * rel_tol * rr0;
+    auto launch_chunk = [&](int chunk) {
+        for (int c = 0; c < chunk; ++c) {
+            k_spmv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.p, w.q, w.scal, w.partial);
+            k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 1);
+            k_update<<<g, TB, 0, st>>>(x, w.r, w.z, w.p, w.q, w.dinv, w.scal, w.partial, n);
+            k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 2);
+            k_pupdate<<<g, TB, 0, st>>>(w.z, w.p, w.scal, n);
+        }
+    };
+    // With `graph`, a full chunk of iterations is captured once as a CUDA
+    // graph and replayed: one launch instead of 5 * check.
+    cudaGraphExec_t exec = nullptr;
+    struct ExecGuard {
+        cudaGraphExec_t &e;
+        ~ExecGuard() {
+            if (e) cudaGraphExecDestroy(e);
+        }
+    } exec_guard{exec};
+    if (graph && max_iter >= check) {
+        cudaGraph_t gr = nullptr;
+        SDOT_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        launch_chunk(check);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(st, &gr);
+        SDOT_CUDA(le);
+        SDOT_CUDA(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&exec, gr, 0);
+        cudaGraphDestroy(gr);
+        SDOT_CUDA(ie);
+    }
     int it = 0;
     while (it < max_iter) {
         const int chunk = check < max_iter - it ? check : max_iter - it;
-        for (int c = 0; c < chunk; ++c) {
-            k_spmv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.p, w.q, w.scal, w.partial);
-            note_launch();
-            k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 1);
-            note_launch();
-            k_update<<<g, TB, 0, st>>>(x, w.r, w.z, w.p, w.q, w.dinv, w.scal, w.partial, n);
-            note_launch();
-            k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 2);
-            note_launch();
-            k_pupdate<<<g, TB, 0, st>>>(w.z, w.p, w.scal, n);
-            note_launch();
-        }
+        if (exec && chunk == check)
+            SDOT_CUDA(cudaGraphLaunch(exec, st));
+        else
+            launch_chunk(chunk);
+        for (int c = 0; c < 5 * chunk; ++c) note_launch();
         SDOT_CUDA(cudaGetLastError());
         it += chunk;
         SDOT_CUDA(cudaMemcpyAsync(hs, w.scal, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -318,13 +341,13 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
 }  // namespace
 
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                    int max_iter, const PcgWork &w, cudaStream_t st, int check) {
-    return pcg_run(RowsMat{rows}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check);
+                    int max_iter, const PcgWork &w, cudaStream_t st, int check, bool graph) {
+    return pcg_run(RowsMat{rows}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check, graph);
 }
 
 PcgResult pcg_solve_csr(const CsrMat &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
                         int max_iter, const PcgWork &w, cudaStream_t st, int check) {
-    return pcg_run(CsrView{A}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check);
+    return pcg_run(CsrView{A}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check, false);
 }
 
 void mass_errors(const double *m, const double *t, long long n, double *partial, double *out, cudaStream_t st) {

@@ -33,8 +33,10 @@ struct PcgResult {
 // gauge_row < 0 disables it.  x starts at 0.  Stops when
 // |r| <= rel_tol |b| or after max_iter iterations (checked every `check`
 // iterations, the only host synchronisations).
+// graph: replay full chunks of `check` iterations from one captured CUDA
+// graph (st must be a created stream).
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                    int max_iter, const PcgWork &w, cudaStream_t st, int check = 32);
+                    int max_iter, const PcgWork &w, cudaStream_t st, int check = 32, bool graph = false);
 
 // The same solve on a CSR matrix (device arrays: off[n + 1], col[nnz], val[nnz]).
 struct CsrMat {

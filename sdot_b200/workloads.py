@@ -27,10 +27,16 @@ def uniform_points(n, dim, rng):
     return rng.random((n, dim))
 
 
-def clustered_points(n, dim, rng, nb_clusters=20, sigma=0.02):
+def clustered_points(n, dim, rng, nb_clusters=20, sigma=0.02, boundary="clamp"):
+    """Isotropic Gaussian clusters (centres uniform); points leaving the unit
+    box are clamped to it (boundary="clamp", the C2 definition) or mirrored
+    back into it (boundary="reflect": no two points coincide)."""
     centres = rng.random((nb_clusters, dim))
     k = np.arange(n) % nb_clusters
     p = centres[k] + sigma * rng.standard_normal((n, dim))
+    if boundary == "reflect":
+        p = np.abs(p)
+        return np.where(p > 1.0, 2.0 - p, p)
     return np.clip(p, 0.0, 1.0)
 
 
@@ -76,7 +82,10 @@ def config4(n=200_000):
 
 
 def serving_requests(count=2000, rate_hz=50.0, seed_salt=0):
-    """Poisson stream of solve requests (C5)."""
+    """Poisson stream of solve requests (C5).  Clustered requests mirror
+    their points at the box faces instead of clamping them: clamping makes
+    coincident Diracs (in 3D, at the box corners), for which no weights
+    reach the target masses."""
     rng = rng_for(5, seed_salt)
     t = np.cumsum(rng.exponential(1.0 / rate_hz, count))
     reqs = []
@@ -85,6 +94,6 @@ def serving_requests(count=2000, rate_hz=50.0, seed_salt=0):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
         clustered = rng.random() < 0.5
         r = np.random.Generator(np.random.PCG64(SEED0 + 5 + 7919 * (k + 1)))
-        p = clustered_points(n, dim, r) if clustered else uniform_points(n, dim, r)
+        p = clustered_points(n, dim, r, boundary="reflect") if clustered else uniform_points(n, dim, r)
         reqs.append({"arrival_s": float(t[k]), "dim": dim, "n": n, "clustered": bool(clustered), "positions": p})
     return reqs
