@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving", action="store_true",
+                    help="serving benchmark: a Poisson stream of OT solves, continuous batching vs sequential")
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--slots", type=int, default=4)
     return ap.parse_args()
 
 
@@ -371,6 +375,17 @@ def run_ours(args):
            "gpu_launches": int(launches1.value - launches0.value),
            "roofline": roofline, "clocks": clk, "wall_timed_s": wall,
            "stages_ms": {"cells": cell}}
+    # ---- outside the timed region: the mixed-precision path on the same
+    # problem (cells/s and its error against the FP64 path) and Newton times
+    if rank == 0 and world == 1:
+        try:
+            out["mixed"] = mixed_leg(L, c, n, dev, flush, args.steps)
+        except Exception as e:  # reported, never required
+            out["mixed"] = {"error": str(e)}
+        try:
+            out["newton"] = newton_leg()
+        except Exception as e:
+            out["newton"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(c)
@@ -384,9 +399,114 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def mixed_leg(L, c, n, dev, flush, steps):
+    """SDOT_MIXED on the bench problem: cells/s timed like `value`, and the
+    largest error of its masses against the FP64 path's, relative to
+    max(|m|, mean mass)."""
+    import torch
+
+    from sdot_b200.power_diagram import PowerDiagram
+
+    g64 = PowerDiagram(c["positions"], c["weights"], precision="fp64")
+    g64.add_box_shape([0, 0], [1, 1])
+    m64 = g64.integrals()
+    g = PowerDiagram(c["positions"], c["weights"], precision="mixed")
+    g.add_box_shape([0, 0], [1, 1])
+    m32 = g.integrals()
+    mean = float(np.abs(m64).mean())
+    err = float((np.abs(m32 - m64) / np.maximum(np.abs(m64), mean)).max())
+    ms = []
+    for k in range(max(3, steps)):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        g.set_positions_and_weights(c["positions"], c["weights"])
+        g.evaluate()
+        ms.append(g.last_timings())
+    tot = [t["tree_ms"] + t["cells_ms"] + t["hessian_ms"] for t in ms[1:]]
+    cells = [t["cells_ms"] for t in ms[1:]]
+    return {"value": n / (float(np.mean(tot)) * 1e-3), "unit": UNIT, "cell_kernel_ms": float(np.mean(cells)),
+            "fp64_redo_cells": int(g.last_overflow_count()), "max_rel_mass_err_vs_fp64": err,
+            "note": "stage times of the same evaluation (tree + cells + Hessian assembly), L2 flushed; "
+                    "host-to-device upload of the Diracs not included"}
+
+
+def newton_leg():
+    """Newton times: C1 (10k, w = 0, to 1e-10) and the 1M C2 positions from w = 0
+    (the given weights leave 43% of the cells empty) to 1e-8, damped, FP64."""
+    from sdot_b200 import workloads
+    from sdot_b200.power_diagram import PowerDiagram
+
+    out = {}
+    for name, c, tol in (("C1_10k_to_1e-10", workloads.config1(), 1e-10),
+                         ("C2_1M_from_w0_to_1e-8", workloads.config2(), 1e-8)):
+        n = len(c["weights"])
+        g = PowerDiagram(c["positions"], np.zeros(n))
+        g.add_box_shape([0, 0], [1, 1])
+        t0 = time.perf_counter()
+        rep = g.solve_weights(np.full(n, 1.0 / n), rel_mass_tol=tol)
+        wall = time.perf_counter() - t0
+        out[name] = {"time_s": wall, "iterations": rep["iterations"], "pcg_iterations": int(rep["pcg_iterations"]),
+                     "evaluations": rep["evaluations"], "max_rel_mass_error": rep["max_rel_mass_error"]}
+    return out
+
+
+# ----------------------------------------------------------------- serving
+def run_stream(reqs, slots, rate_scale, tol):
+    """Submits the requests at their arrival times (arrival_s * rate_scale) to a
+    server with `slots` slots; returns per-request latencies (s) and reports."""
+    from sdot_b200.serving import Server
+
+    srv = Server(slots=slots, hbm_budget_bytes=64 << 30, rel_mass_tol=tol)
+    ids = []
+    t0 = time.perf_counter()
+    for r in reqs:
+        due = r["arrival_s"] * rate_scale
+        delay = due - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(r["positions"], np.full(r["n"], 1.0 / r["n"])))
+    srv.drain()
+    wall = time.perf_counter() - t0
+    reps = [srv.result(i)[1] for i in ids]
+    srv.close()
+    lat = np.array([(rp["end_ms"] - rp["submit_ms"]) * 1e-3 for rp in reps])
+    return lat, reps, wall
+
+
+def run_serving(args):
+    """C5: Poisson stream of 2D/3D OT solves (n log-uniform in [1e3, 2e5]),
+    unit box, targets 1/n, relative mass tolerance 1e-8.  First the
+    sequential service rate is measured (all requests back to back, 1 slot):
+    that is the saturation rate.  Then the stream arrives at 0.8 of it and is
+    served twice: one request at a time (sequential plain solves) and by the
+    continuously batched server; p50/p99 latency = completion - arrival."""
+    from sdot_b200 import workloads
+
+    tol = 1e-8
+    reqs = workloads.serving_requests(count=args.requests, rate_hz=1.0)
+    lat0, reps0, wall0 = run_stream(reqs, 1, 0.0, tol)
+    sat = len(reqs) / wall0
+    rate = 0.8 * sat
+    scale = 1.0 / rate  # arrival_s was drawn at 1 request/s
+    out = {"metric": "served OT solve latency (p50/p99), Poisson arrivals at 0.8 x the sequential saturation rate",
+           "unit": "s", "requests": len(reqs), "saturation_rate_hz": sat, "arrival_rate_hz": rate,
+           "tolerance": tol, "dims": {"2d": sum(r["dim"] == 2 for r in reqs), "3d": sum(r["dim"] == 3 for r in reqs)},
+           "diracs_total": int(sum(r["n"] for r in reqs)), "data": "synthetic (seeded C5 stream)"}
+    for name, slots in (("sequential", 1), ("batched", args.slots)):
+        lat, reps, wall = run_stream(reqs, slots, scale, tol)
+        out[name] = {"slots": slots, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                     "mean_s": float(lat.mean()), "throughput_hz": len(reqs) / wall,
+                     "max_rel_mass_error": float(max(r["max_rel_mass_error"] for r in reps)),
+                     "failed": int(sum(r["status"] != 0 for r in reps))}
+    out["p99_speedup"] = out["sequential"]["p99_s"] / out["batched"]["p99_s"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.serving:
+        run_serving(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

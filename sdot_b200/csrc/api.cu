@@ -129,10 +129,17 @@ struct sdot_ctx {
     Rows rows, nb;             // Hessian rows, boundary id lists (sorted order)
     long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
     int *ovf_list = nullptr, *ovf_cnt = nullptr;
+    int *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;  // 3D: third pass
+    void *scratch3 = nullptr;                        // 3D: third pass faces
     unsigned *err = nullptr;
     int *guard = nullptr;
     long long item_nv = 0;
+    std::vector<int> item_off_h;  // vertex offsets of the shapes (several shapes)
     void *scratch = nullptr, *scan_tmp = nullptr;
+    // several shapes: one cell pass per shape into these, summed into the above
+    Rows rows_tmp;
+    double *t_mass = nullptr, *t_mass_c = nullptr, *t_ctd = nullptr, *s_mom = nullptr;
+    long long mcap = 0;
     long long nnz = 0, nb_total = 0;
     long long n_void = 0;
     int last_ovf = 0;
@@ -149,6 +156,7 @@ struct sdot_ctx {
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
         free_eval();
         free_newton();
+        free_multi();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -158,7 +166,9 @@ struct sdot_ctx {
         free_rows(rows);
         free_rows(nb);
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
-        dfree(ovf_list); dfree(ovf_cnt); dfree(err); dfree(guard);
+        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err); dfree(guard);
+        if (scratch3) cudaFree(scratch3);
+        scratch3 = nullptr;
         if (scratch) cudaFree(scratch);
         if (scan_tmp) cudaFree(scan_tmp);
         scratch = scan_tmp = nullptr;
@@ -198,6 +208,11 @@ struct sdot_ctx {
         dalloc(offsets, ecap + 1);
         dalloc(ovf_list, ecap);
         dalloc(ovf_cnt, 1);
+        if (dim == 3) {
+            dalloc(ovf_list2, ecap);
+            dalloc(ovf_cnt2, 1);
+            SDOT_CUDA(cudaMalloc(&scratch3, cells3d_scratch_bytes()));
+        }
         dalloc(err, 1);
         dalloc(guard, 3);
         SDOT_CUDA(cudaMalloc(&scratch, cells2d_scratch_bytes()));
@@ -246,6 +261,10 @@ struct sdot_ctx {
             dalloc(d_start, 8);
             SDOT_CUDA(cudaMemcpyAsync(d_start, eb.xy.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream));
             item_nv = off.back();
+            item_off_h = off;
+            for (size_t k = 0; k + 1 < off.size(); ++k)
+                if (off[k + 1] - off[k] > CAP_FAST_2D)
+                    throw Unsupported("a domain shape has more vertices than the cell capacity");
             dalloc(d_item_off, off.size());
             SDOT_CUDA(cudaMemcpyAsync(d_item_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
             dalloc(d_item_xy, xy.size());
@@ -302,9 +321,49 @@ struct sdot_ctx {
             return;
         }
         upload_domain();
-        if (mode == DM_MULTI)
-            throw Unsupported("domains made of several shapes are not enabled in this build (the multi-shape "
-                              "cell kernel is disabled); use one shape or an image density");
+    }
+
+    void reserve_multi() {
+        if (mcap >= n && t_mass) return;
+        free_multi();
+        mcap = std::max<long long>(n, 1);
+        alloc_rows(rows_tmp, mcap, ROWCAP_2D, true);
+        dalloc(t_mass, mcap); dalloc(t_mass_c, mcap); dalloc(t_ctd, 2 * mcap); dalloc(s_mom, 2 * mcap);
+    }
+    void free_multi() {
+        free_rows(rows_tmp);
+        dfree(t_mass); dfree(t_mass_c); dfree(t_ctd); dfree(s_mom);
+        mcap = 0;
+    }
+
+    // ConvexPolyhedronAssembly::for_each_intersection (ConvexPolyhedronAssembly.tcc:132-142)
+    // sums over the shapes the integrals of cell ∩ shape.  Here: one cell
+    // pass per shape, with the shape itself as the starting polygon (the
+    // cell ∩ shape is the same convex set), summed: masses and centroid
+    // moments added, Hessian rows appended (equal columns are merged by the
+    // row assembly, as the reference merges its per-piece entries).
+    void evaluate_multi() {
+        reserve_multi();
+        SDOT_CUDA(cudaMemsetAsync(s_mass, 0, size_t(n) * sizeof(double), stream));
+        SDOT_CUDA(cudaMemsetAsync(s_mass_c, 0, size_t(n) * sizeof(double), stream));
+        SDOT_CUDA(cudaMemsetAsync(s_mom, 0, size_t(2 * n) * sizeof(double), stream));
+        rows_clear(rows, n, stream);
+        SDOT_CUDA(cudaMemsetAsync(rows.side_used, 0, sizeof(unsigned long long), stream));
+        for (size_t k = 0; k + 1 < item_off_h.size(); ++k) {
+            Cell2DArgs a = args();
+            a.mode = DM_SINGLE;
+            a.start_n = item_off_h[k + 1] - item_off_h[k];
+            a.start_xy = d_item_xy + 2 * item_off_h[k];
+            a.coeff = items[k].coeff;
+            a.mass = t_mass;
+            a.mass_c = t_mass_c;
+            a.ctd = t_ctd;
+            a.rows = rows_tmp;
+            cells2d_launch(a, scratch, stream);
+            accum_pass2(s_mass, s_mass_c, s_mom, t_mass, t_mass_c, t_ctd, n, stream);
+            rows_append(rows, rows_tmp, n, err, stream);
+        }
+        centroids_final2(s_ctd, s_mom, s_mass_c, n, stream);
     }
 
     Cell3DArgs args3() {
@@ -321,6 +380,8 @@ struct sdot_ctx {
         a.coeff = boxes3[0].coeff;
         a.ovf_list = ovf_list;
         a.ovf_cnt = ovf_cnt;
+        a.ovf_list2 = ovf_list2;
+        a.ovf_cnt2 = ovf_cnt2;
         a.err = err;
         a.guard = guard;
         return a;
@@ -361,9 +422,11 @@ struct sdot_ctx {
             a.mass = s_mass;
             a.ctd = s_ctd;
             a.rows = rows;
-            cells3d_launch(a, stream);
+            cells3d_launch(a, scratch3, stream);
             // get_centroids' mass is the integral itself in 3D
             SDOT_CUDA(cudaMemcpyAsync(s_mass_c, s_mass, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        } else if (mode == DM_MULTI) {
+            evaluate_multi();
         } else {
             Cell2DArgs a = args();
             a.mass = s_mass;
@@ -387,8 +450,26 @@ struct sdot_ctx {
         SDOT_CUDA(cudaEventElapsedTime(&times[0], ev[0], ev[1]));
         SDOT_CUDA(cudaEventElapsedTime(&times[1], ev[1], ev[2]));
         SDOT_CUDA(cudaEventElapsedTime(&times[2], ev[2], ev[3]));
+        if ((last_err & DE_SIDE) && side_retries < 4) {
+            // long rows outgrew the side buffer: grow it and evaluate again
+            ++side_retries;
+            grow_side(rows);
+            if (dim != 3 && mode == DM_MULTI) grow_side(rows_tmp);
+            const int st = evaluate();
+            side_retries = 0;
+            return st;
+        }
         eval_dirty = false;
         return finish_status();
+    }
+
+    int side_retries = 0;
+    // a side buffer four times larger (the ELL part is kept)
+    static void grow_side(Rows &r) {
+        if (!r.side_col) return;
+        r.side_cap *= 4;
+        dalloc(r.side_col, r.side_cap);
+        if (r.side_val) dalloc(r.side_val, r.side_cap);
     }
 
     int finish_status() {
@@ -397,9 +478,12 @@ struct sdot_ctx {
             return SDOT_ITER_CAP;
         }
         if (last_err & DE_CAPACITY) {
-            last_error = dim == 3 ? "a cell exceeded the maximum polyhedron capacity (64 faces of 32 vertices) or "
-                                    "the long-row buffer"
-                                  : "a cell exceeded the maximum polygon capacity (1024 vertices) or the long-row buffer";
+            last_error = dim == 3 ? "a cell exceeded the maximum polyhedron capacity (128 faces of 64 vertices)"
+                                  : "a cell exceeded the maximum polygon capacity (1024 vertices)";
+            return SDOT_CAPACITY;
+        }
+        if (last_err & DE_SIDE) {
+            last_error = "long Hessian rows or neighbour lists exceeded the side buffer after it was grown";
             return SDOT_CAPACITY;
         }
         if (last_err & DE_DEGEN) {
@@ -423,15 +507,28 @@ struct sdot_ctx {
         evaluate();
         if (!nb.cnt || nb.stride < ecap) alloc_rows(nb, ecap, dim == 3 ? NBCAP_3D : NBCAP_2D, false);
         if (!nb_offsets) dalloc(nb_offsets, ecap + 1);
-        SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
-        if (dim == 3) {
-            Cell3DArgs a = args3();
-            a.nb = nb;
-            cells3d_launch(a, stream);
-        } else {
-            Cell2DArgs a = args();
-            a.nb = nb;
-            cells2d_launch(a, scratch, stream);
+        for (int attempt = 0;; ++attempt) {
+            SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
+            if (dim == 3) {
+                Cell3DArgs a = args3();
+                a.nb = nb;
+                cells3d_launch(a, scratch3, stream);
+            } else {
+                // several shapes: the cut ids of the traversal cell in the
+                // englobing box (the cell the reference's callback receives)
+                Cell2DArgs a = args();
+                if (mode == DM_MULTI) {
+                    a.mode = DM_SINGLE;
+                    a.coeff = 1.0;
+                }
+                a.nb = nb;
+                cells2d_launch(a, scratch, stream);
+            }
+            unsigned e = 0;
+            SDOT_CUDA(cudaMemcpyAsync(&e, err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            SDOT_CUDA(cudaStreamSynchronize(stream));
+            if (!(e & DE_SIDE) || attempt >= 4) break;
+            grow_side(nb);  // long id lists outgrew the side buffer
         }
         nb_counts(nb, n, perm(), cnt_orig, stream);
         scan_exclusive_total<long long>(cnt_orig, nb_offsets, n, scan_tmp, stream);

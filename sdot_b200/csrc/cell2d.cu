@@ -33,7 +33,7 @@ namespace sdot {
 
 namespace {
 
-constexpr int T2D = 64;     // threads per block of the fast kernel
+constexpr int T2D_MAX = 128;  // largest block of the fast kernels (their block size is tuned, see launch_all)
 constexpr int STACK = 64;   // traversal stack (depth <= 17 levels, <= 3 pending siblings each)
 constexpr int WTIER_WARPS = 148 * 4;  // warps of the warp-per-cell tier (4 per SM)
 
@@ -196,11 +196,6 @@ struct NbSink {
 template <class Stage, class P>
 SDOT_HDI void stream_cell(const P &cell, int n, Stage &st) {
     for (int k = 0; k < n; ++k) st.push(cell.X(k), cell.Y(k), k);
-    st.finish();
-}
-template <class Stage>
-SDOT_HDI void stream_piece(const PolyView<double> &piece, int n, Stage &st) {
-    for (int k = 0; k < n; ++k) st.push(piece.X(k), piece.Y(k), piece.I(k));
     st.finish();
 }
 
@@ -515,6 +510,7 @@ struct ReclipView {
     PolyView<float> poly;
     int n;
     double c0x, c0y, w0;
+    int cap = CAP_FAST_2D;  // vertex slots (bound of the debug checks)
     mutable int ck = -1;
     mutable double vx = 0, vy = 0;
 
@@ -567,8 +563,8 @@ struct ReclipView {
     // length (a reversed or vanishing edge marks a vertex where four cells
     // nearly meet, whose topology depends on rounding).
     SDOT_HDI bool consistent() const {
-        double vx0 = 0, vy0 = 0, px = 0, py = 0, scale = 0;
-        float fx0 = 0, fy0 = 0, gx = 0, gy = 0;
+        double vx0 = 0, vy0 = 0, px = 0, py = 0;
+        float gx = 0, gy = 0;
         for (int k = 0; k <= n && n >= 2; ++k) {
             const int kk = k == n ? 0 : k;
             double ux, uy;
@@ -582,12 +578,9 @@ struct ReclipView {
             const float fx = poly.X(kk), fy = poly.Y(kk);
             const double sc = fabs(double(fx)) + fabs(double(fy)) + 1e-300;
             if (!(fabs(ux - fx) + fabs(uy - fy) <= 1e-4 * sc)) return false;
-            scale = fmax(scale, sc);
             if (k == 0) {
                 vx0 = ux;
                 vy0 = uy;
-                fx0 = fx;
-                fy0 = fy;
             } else {
                 const double ex = ux - px, ey = uy - py;
                 const double fex = double(fx) - gx, fey = double(fy) - gy;
@@ -599,9 +592,6 @@ struct ReclipView {
             gx = fx;
             gy = fy;
         }
-        (void)fx0;
-        (void)fy0;
-        (void)scale;
         return true;
     }
 };
@@ -611,8 +601,8 @@ struct ReclipView {
 // was exceeded (the cell is then rebuilt by the next tier, which rewrites
 // every output of it).
 template <int MODE, bool BALL, class P>
-SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n, int cap, double *acc, int acc_st,
-                          const PolyView<double> &piece, Out &row, Out &nbo) {
+SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n, double *acc, int acc_st, Out &row,
+                          Out &nbo) {
     const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
     if (n == -2) {
         // failed guard: report a NaN cell, not an overflow
@@ -698,32 +688,6 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
                         }
                     }
                 }
-            } else {  // DM_MULTI
-                for (int it = 0; it < A.nitems; ++it) {
-                    int np = n;
-                    for (int k = 0; k < n; ++k) {
-                        piece.X(k) = cell.X(k);
-                        piece.Y(k) = cell.Y(k);
-                        piece.I(k) = k;
-                    }
-                    if (A.item_off[it] < 0 || A.item_off[it + 1] > A.item_nv) {
-                        guard_fail(A, 3, s, it);
-                        continue;
-                    }
-                    for (int e = A.item_off[it]; e < A.item_off[it + 1] && np > 0; ++e)
-                        np = plane_cut(piece, np, cap, A.item_xy[2 * e], A.item_xy[2 * e + 1], A.item_nrm[2 * e],
-                                       A.item_nrm[2 * e + 1], PID_OWN, false);
-                    if (np < 0) return false;
-                    sink.begin_piece(A.item_coeff[it]);
-                    if (BALL) {
-                        DiscClip<SinkT> dc(sink, c0x, c0y, r);
-                        stream_piece(piece, np, dc);
-                        sink.end_piece(dc.result_radius());
-                    } else {
-                        stream_piece(piece, np, sink);
-                        sink.end_piece(-1.0);
-                    }
-                }
             }
         }
         if (A.rows.cnt) {
@@ -770,32 +734,30 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
     return true;
 }
 
-// shared memory of the fast kernel, in half-doubles per vertex slot and
-// thread beyond x, y, id: acc (image, multi) and the piece polygon (multi)
+// shared memory of the fast kernels, in half-doubles per vertex slot and
+// thread beyond the polygon: the per-edge accumulators of the image mode
 template <int MODE>
 constexpr int smem_extra_halves() {
-    return MODE == DM_SINGLE ? 0 : (MODE == DM_IMAGE ? 2 : 8);
+    return MODE == DM_IMAGE ? 2 : 0;
 }
 
 template <int MODE, bool BALL>
-__global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
+__global__ void __launch_bounds__(T2D_MAX) k_cells2d(const Cell2DArgs A) {
     extern __shared__ double smem[];
     constexpr int CAP = CAP_FAST_2D;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, T2D = blockDim.x;
     double *sx = smem;
     double *sy = sx + CAP * T2D;
     int *sid = reinterpret_cast<int *>(sy + CAP * T2D);
     double *extra = sy + CAP * T2D + (CAP * T2D + 1) / 2;
     PolyView<double> cell{sx + t, sy + t, sid + t, T2D, CAP};
     double *acc = extra + t;
-    PolyView<double> piece{extra + CAP * T2D + t, extra + 2 * CAP * T2D + t,
-                           reinterpret_cast<int *>(extra + 3 * CAP * T2D) + t, T2D, CAP};
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
     const int n = build_cell(A, s, cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s]);
     Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
     Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
-    if (finish_cell<MODE, BALL>(A, s, cell, n, CAP, acc, T2D, piece, row, nbo)) {
+    if (finish_cell<MODE, BALL>(A, s, cell, n, acc, T2D, row, nbo)) {
         if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
         if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
     } else {
@@ -809,17 +771,16 @@ __global__ void __launch_bounds__(T2D) k_cells2d(const Cell2DArgs A) {
 // whose FP32 decisions were too close to call, whose topology does not
 // re-clip cleanly, or that overflow the capacity go to the FP64 warp tier.
 template <int MODE, bool BALL>
-__global__ void __launch_bounds__(T2D) k_cells2d_mixed(const Cell2DArgs A) {
+__global__ void __launch_bounds__(T2D_MAX) k_cells2d_mixed(const Cell2DArgs A) {
     extern __shared__ double smem[];
     constexpr int CAP = CAP_FAST_2D;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, T2D = blockDim.x;
     float *sx = reinterpret_cast<float *>(smem);
     float *sy = sx + CAP * T2D;
     int *sid = reinterpret_cast<int *>(sy + CAP * T2D);
     double *extra = reinterpret_cast<double *>(sid + CAP * T2D);
     PolyView<float> cell{sx + t, sy + t, sid + t, T2D, CAP};
     double *acc = extra + t;
-    const PolyView<double> no_piece{nullptr, nullptr, nullptr, T2D, 0};  // several shapes never take this path
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
     const double c0x = A.pos[2 * s], c0y = A.pos[2 * s + 1], w0 = A.w[s];
@@ -835,7 +796,7 @@ __global__ void __launch_bounds__(T2D) k_cells2d_mixed(const Cell2DArgs A) {
         Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride,
                 A.rows.cap);
         Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
-        ok = finish_cell<MODE, BALL>(A, s, view, n, CAP, acc, T2D, no_piece, row, nbo);
+        ok = finish_cell<MODE, BALL>(A, s, view, n, acc, T2D, row, nbo);
         if (ok) {
             if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
             if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
@@ -850,7 +811,7 @@ __global__ void __launch_bounds__(T2D) k_cells2d_mixed(const Cell2DArgs A) {
 // Polygon, accumulators and row buffers of one warp of the warp tier,
 // contiguous (vertex k at index k) so that the lanes read 32 vertices at once.
 struct WarpScratch {
-    PolyView<double> cell, piece;
+    PolyView<double> cell;
     double *acc, *row_val;
     int *row_col, *nb_id;
     __device__ WarpScratch(double *base, int cap) {
@@ -859,8 +820,6 @@ struct WarpScratch {
         p += 3 * cap;
         acc = p;
         p += cap;
-        piece = PolyView<double>{p, p + cap, reinterpret_cast<int *>(p + 2 * cap), 1, cap};
-        p += 3 * cap;
         row_val = p;
         p += cap + 1;
         row_col = reinterpret_cast<int *>(p);
@@ -868,10 +827,10 @@ struct WarpScratch {
         nb_id = reinterpret_cast<int *>(p);  // 2 cap ints
     }
 };
-// doubles of one warp's scratch: cell (3 cap), acc (cap), piece (3 cap), row
-// values (cap + 1), row columns (cap + 1), ids (2 cap ints), rounded up
+// doubles of one warp's scratch: cell (3 cap), acc (cap), row values (cap + 1),
+// row columns (cap + 1), ids (2 cap ints), rounded up
 __host__ __device__ constexpr long long warp_scratch_doubles(int cap) {
-    return (8LL * cap + 2LL * (cap + 1) + 31) / 32 * 32;
+    return (5LL * cap + 2LL * (cap + 1) + 31) / 32 * 32;
 }
 
 // Copies a finished row from scratch to its ELL slot or the side buffer.
@@ -883,7 +842,7 @@ __device__ bool commit(const Rows &R, long long s, const int *col, const double 
         }
     } else {
         const unsigned long long off = atomicAdd(R.side_used, (unsigned long long)cnt);
-        if ((long long)(off + cnt) > R.side_cap) return false;
+        if ((long long)(off + cnt) > R.side_cap) return false;  // the caller flags DE_SIDE
         R.side[s] = (long long)off;
         for (int k = 0; k < cnt; ++k) {
             R.side_col[off + k] = col[k * st];
@@ -1009,11 +968,12 @@ __global__ void __launch_bounds__(128) k_cells2d_wtier(const Cell2DArgs A, doubl
         if (lane == 0) {
             Out row(A.rows.cnt ? W.row_col : nullptr, W.row_val, 1, CAP + 1);
             Out nbo(A.nb.cnt ? W.nb_id : nullptr, nullptr, 1, 2 * CAP);
-            bool ok = finish_cell<MODE, BALL>(A, s, W.cell, n, CAP, W.acc, 1, W.piece, row, nbo);
+            const bool built = finish_cell<MODE, BALL>(A, s, W.cell, n, W.acc, 1, row, nbo);
+            bool ok = built;
             if (ok && A.rows.cnt) ok = commit(A.rows, s, W.row_col, W.row_val, 1, row.cnt);
             if (ok && A.nb.cnt) ok = commit(A.nb, s, W.nb_id, nullptr, 1, nbo.cnt);
             if (!ok) {
-                atomicOr(A.err, DE_CAPACITY);
+                atomicOr(A.err, built ? DE_SIDE : DE_CAPACITY);
                 if (A.mass) A.mass[s] = nan("");
                 if (A.rows.cnt) A.rows.cnt[s] = 0;
                 if (A.nb.cnt) A.nb.cnt[s] = 0;
@@ -1023,24 +983,73 @@ __global__ void __launch_bounds__(128) k_cells2d_wtier(const Cell2DArgs A, doubl
     }
 }
 
+// Block size of the fast kernels, picked once per kernel variant on the
+// device by timing the candidates on the first evaluation large enough to
+// tell them apart (the results do not depend on it: one thread builds one
+// cell whatever the block).
+struct BlockTuner {
+    int best = 0;
+};
+
 template <int MODE, bool BALL>
-void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
+size_t fast_smem(int bs, bool mixed) {
     constexpr int CAP = CAP_FAST_2D;
-    const size_t smem = size_t(CAP) * T2D * 16 + size_t(CAP * T2D + 1) / 2 * 8 +
-                        size_t(smem_extra_halves<MODE>()) * CAP * T2D * 4;
-    static bool attr_set = false;
-    if (!attr_set) {
-        SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr_set = true;
-    }
-    if (MODE != DM_MULTI && a.mixed) {
-        const size_t smem_m = size_t(CAP) * T2D * 12 + size_t(smem_extra_halves<MODE>()) * CAP * T2D * 4;
-        k_cells2d_mixed<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem_m, st>>>(a);
-    } else {
-        k_cells2d<MODE, BALL><<<ceil_div(a.n, T2D), T2D, smem, st>>>(a);
-    }
+    const size_t extra = size_t(smem_extra_halves<MODE>()) * CAP * bs * 4;
+    return mixed ? size_t(CAP) * bs * 12 + extra : size_t(CAP) * bs * 16 + size_t(CAP * bs + 1) / 2 * 8 + extra;
+}
+
+template <int MODE, bool BALL>
+void launch_fast(const Cell2DArgs &a, int bs, cudaStream_t st) {
+    const size_t smem = fast_smem<MODE, BALL>(bs, a.mixed != 0);
+    if (a.mixed)
+        k_cells2d_mixed<MODE, BALL><<<ceil_div(a.n, bs), bs, smem, st>>>(a);
+    else
+        k_cells2d<MODE, BALL><<<ceil_div(a.n, bs), bs, smem, st>>>(a);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
+}
+
+template <int MODE, bool BALL>
+void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(fast_smem<MODE, BALL>(T2D_MAX, false))));
+        SDOT_CUDA(cudaFuncSetAttribute(k_cells2d_mixed<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(fast_smem<MODE, BALL>(T2D_MAX, true))));
+        attr_set = true;
+    }
+    static BlockTuner tuner[2];  // FP64, mixed
+    BlockTuner &tu = tuner[a.mixed ? 1 : 0];
+    if (!tu.best) {
+        if (a.n >= (1 << 17)) {
+            // time each candidate on this evaluation's cells; the outputs of
+            // the trial runs are all rewritten by the run that follows
+            const int cand[3] = {32, 64, 128};
+            float best_ms = 0;
+            cudaEvent_t e0, e1;
+            SDOT_CUDA(cudaEventCreate(&e0));
+            SDOT_CUDA(cudaEventCreate(&e1));
+            for (int bs : cand) {
+                SDOT_CUDA(cudaEventRecord(e0, st));
+                launch_fast<MODE, BALL>(a, bs, st);
+                SDOT_CUDA(cudaEventRecord(e1, st));
+                SDOT_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                SDOT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (!tu.best || ms < best_ms) {
+                    tu.best = bs;
+                    best_ms = ms;
+                }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+            if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
+            if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
+        }
+    }
+    launch_fast<MODE, BALL>(a, tu.best ? tu.best : 64, st);
     k_cells2d_wtier<MODE, BALL><<<WTIER_WARPS / 4, 128, 0, st>>>(a, static_cast<double *>(scratch), WTIER_WARPS,
                                                                   a.ovf_list, a.ovf_cnt);
     note_launch();
@@ -1072,7 +1081,7 @@ void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
     } else if (a.mode == DM_IMAGE) {
         if (ball) launch_all<DM_IMAGE, true>(a, scratch, st); else launch_all<DM_IMAGE, false>(a, scratch, st);
     } else {
-        if (ball) launch_all<DM_MULTI, true>(a, scratch, st); else launch_all<DM_MULTI, false>(a, scratch, st);
+        throw CudaError{cudaErrorInvalidValue, "cells2d_launch: a domain of several shapes runs one pass per shape"};
     }
 }
 

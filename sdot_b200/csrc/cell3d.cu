@@ -25,6 +25,8 @@
 //    diagonal their sum; domain faces skipped (get_der_integrals_wrt_weights.h:43-88).
 #include "cell3d.cuh"
 
+#include <type_traits>
+
 namespace sdot {
 
 namespace {
@@ -59,20 +61,28 @@ struct Cell3 {
 __device__ inline double shfl(double v, int src) { return __shfl_sync(FULL, v, src); }
 
 // Outcome of a cut: 0 done, 1 a capacity was exceeded, 2 degenerate geometry.
+// bit masks over the vertices of one face
+__device__ inline int popc_m(unsigned m) { return __popc(m); }
+__device__ inline int popc_m(unsigned long long m) { return __popcll(m); }
+__device__ inline int ffs_m(unsigned m) { return __ffs(int(m)); }
+__device__ inline int ffs_m(unsigned long long m) { return __ffsll((long long)m); }
+
 template <int FPL, int MAXV>
 __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double qb, int qid) {
+    using Mask = typename std::conditional<(MAXV > 32), unsigned long long, unsigned>::type;
+    constexpr int MB = 8 * sizeof(Mask);
     const int lane = threadIdx.x & 31;
     auto &F = C.F;
-    unsigned mask[FPL];
+    Mask mask[FPL];
     bool has = false;
 #pragma unroll
     for (int r = 0; r < FPL; ++r) {
         const int f = lane + 32 * r;
-        unsigned m = 0;
+        Mask m = 0;
         for (int v = 0; v < C.nv[r]; ++v) {
             const int i = F.at(v, f);
             const double d = qb - (qx * F.X[i] + qy * F.Y[i] + qz * F.Z[i]);
-            m |= unsigned(d < 0.0) << v;
+            m |= Mask(d < 0.0) << v;
         }
         mask[r] = m;
         has |= m != 0;
@@ -91,23 +101,23 @@ __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double
         ex[r] = ey[r] = ez[r] = 0;
         const int n = C.nv[r];
         if (n == 0 || mask[r] == 0) continue;
-        const unsigned full = n >= 32 ? FULL : ((1u << n) - 1u);
-        const unsigned outs = mask[r] & full;
+        const Mask full = n >= MB ? ~Mask(0) : ((Mask(1) << n) - 1);
+        const Mask outs = mask[r] & full;
         if (outs == full) {  // the whole face is removed
             C.nv[r] = 0;
             continue;
         }
         // out vertex k whose predecessor is in: the start of the outside run
-        const unsigned prev_out = ((outs << 1) | (outs >> (n - 1))) & full;  // bit k: vertex k - 1 is out
-        const unsigned starts = outs & ~prev_out;
-        const unsigned next_out = ((outs >> 1) | (outs << (n - 1))) & full;  // bit k: vertex k + 1 is out
-        const unsigned ends = outs & ~next_out;
-        if (__popc(starts) != 1 || __popc(ends) != 1) {
+        const Mask prev_out = ((outs << 1) | (outs >> (n - 1))) & full;  // bit k: vertex k - 1 is out
+        const Mask starts = outs & ~prev_out;
+        const Mask next_out = ((outs >> 1) | (outs << (n - 1))) & full;  // bit k: vertex k + 1 is out
+        const Mask ends = outs & ~next_out;
+        if (popc_m(starts) != 1 || popc_m(ends) != 1) {
             bad = true;
             continue;
         }
-        const int o1 = __ffs(starts) - 1, o2 = __ffs(ends) - 1;
-        const int nout = __popc(outs);
+        const int o1 = ffs_m(starts) - 1, o2 = ffs_m(ends) - 1;
+        const int nout = popc_m(outs);
         const int il = o1 == 0 ? n - 1 : o1 - 1;  // last inside vertex before the run
         const int fi = o2 == n - 1 ? 0 : o2 + 1;  // first inside vertex after it
         const int nn = n - nout + 2;
@@ -481,7 +491,7 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
             nnb += __popc(nm);
         }
     }
-    bool ok = true;
+    bool ok = true;  // the rows fit the side buffer
     if (status == 0) {
         const double mass = A.coeff * vol;
         if (lane == 0) {
@@ -499,7 +509,7 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
     }
     if (status == 2 || !ok) {
         if (lane == 0) {
-            flag_error(A.err, status == 2 ? DE_DEGEN : DE_CAPACITY);
+            flag_error(A.err, status == 2 ? DE_DEGEN : DE_SIDE);
             if (A.mass) A.mass[s] = nan("");
             if (A.ctd) A.ctd[3 * s] = A.ctd[3 * s + 1] = A.ctd[3 * s + 2] = nan("");
             if (A.rows.cnt) {
@@ -514,15 +524,17 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
     return 0;
 }
 
+// The faces of a warp live in shared memory, or, for the largest capacity,
+// in global scratch (gscratch != null: WB bytes per warp).
 template <int FPL, int MAXV>
 __global__ void __launch_bounds__(64) k_cells3d(const Cell3DArgs A, const int *list, const int *list_cnt,
-                                                int *next_list, int *next_cnt, int nwarps) {
+                                                int *next_list, int *next_cnt, int nwarps, char *gscratch) {
     extern __shared__ double smem3[];
     constexpr int MAXF = 32 * FPL;
     constexpr size_t WB = warp_smem_bytes<FPL, MAXV>();
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
-    char *base = reinterpret_cast<char *>(smem3) + WB * wib;
+    char *base = gscratch ? gscratch + WB * size_t(gw) : reinterpret_cast<char *>(smem3) + WB * wib;
     Cell3<FPL, MAXV> C;
     C.F.X = reinterpret_cast<double *>(base);
     C.F.Y = C.F.X + MAXV * MAXF;
@@ -554,34 +566,40 @@ __global__ void __launch_bounds__(64) k_cells3d(const Cell3DArgs A, const int *l
 
 template <int FPL, int MAXV, int WPB>
 void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *next_list, int *next_cnt, long long ncells,
-             cudaStream_t st) {
-    constexpr size_t smem = warp_smem_bytes<FPL, MAXV>() * WPB;
+             char *gscratch, long long max_blocks, cudaStream_t st) {
+    const size_t smem = gscratch ? 0 : warp_smem_bytes<FPL, MAXV>() * WPB;
     static bool attr = false;
-    if (!attr) {
+    if (!attr && !gscratch) {
         SDOT_CUDA(cudaFuncSetAttribute(k_cells3d<FPL, MAXV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         attr = true;
     }
-    const long long max_blocks = 148LL * (FPL == 1 ? 7 : 3);
     long long blocks = (ncells + WPB - 1) / WPB;
     if (blocks > max_blocks) blocks = max_blocks;
     if (blocks < 1) blocks = 1;
     k_cells3d<FPL, MAXV><<<int(blocks), 32 * WPB, smem, st>>>(a, list, list_cnt, next_list, next_cnt,
-                                                               int(blocks) * WPB);
+                                                               int(blocks) * WPB, gscratch);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
 
+constexpr long long G3_WARPS = 148;  // warps of the global-memory pass
+
 }  // namespace
 
-void cells3d_launch(const Cell3DArgs &a, cudaStream_t st) {
+size_t cells3d_scratch_bytes() { return warp_smem_bytes<4, 64>() * G3_WARPS + 256; }
+
+void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st) {
     if (a.n == 0) return;
     SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt2, 0, sizeof(int), st));
     if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
     if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
-    launch3<1, 16, 2>(a, nullptr, nullptr, a.ovf_list, a.ovf_cnt, a.n, st);
-    // the large pass takes the overflow list (its length is on the device:
-    // every resident warp of the launch checks it)
-    launch3<2, 32, 1>(a, a.ovf_list, a.ovf_cnt, nullptr, nullptr, 148LL * 3, st);
+    launch3<1, 16, 2>(a, nullptr, nullptr, a.ovf_list, a.ovf_cnt, a.n, nullptr, 148LL * 7, st);
+    // the larger passes take the overflow lists (their lengths are on the
+    // device: every warp of the launch reads them)
+    launch3<2, 32, 1>(a, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2, 148LL * 3, nullptr, 148LL * 3, st);
+    launch3<4, 64, 1>(a, a.ovf_list2, a.ovf_cnt2, nullptr, nullptr, G3_WARPS, static_cast<char *>(scratch), G3_WARPS,
+                      st);
 }
 
 }  // namespace sdot

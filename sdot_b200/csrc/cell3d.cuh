@@ -24,14 +24,19 @@ struct Cell3DArgs {
     double *ctd = nullptr;   // 3n
     Rows rows;               // Hessian rows (rows.cnt null: skipped)
     Rows nb;                 // neighbour ids (nb.cnt null: skipped)
-    int *ovf_list = nullptr;  // cells handed to the large-capacity pass
+    int *ovf_list = nullptr;  // cells handed to the second pass
     int *ovf_cnt = nullptr;
+    int *ovf_list2 = nullptr;  // cells handed to the third pass
+    int *ovf_cnt2 = nullptr;
     unsigned *err = nullptr;
     int *guard = nullptr;
 };
 
-// First pass over every cell (up to 32 faces of 16 vertices), then the cells
-// that overflowed it (up to 64 faces of 32 vertices).
-void cells3d_launch(const Cell3DArgs &a, cudaStream_t st);
+// First pass over every cell (up to 32 faces of 16 vertices, shared memory),
+// then the cells that overflowed it (64 faces of 32 vertices, shared memory),
+// then those that overflowed again (128 faces of 64 vertices, in `scratch`
+// of cells3d_scratch_bytes() bytes).
+size_t cells3d_scratch_bytes();
+void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st);
 
 }  // namespace sdot

@@ -103,6 +103,7 @@ enum DevErr : unsigned {
     DE_PIECE = 8u,         // a piece overflowed its capacity
     DE_GUARD = 16u,        // an input failed a consistency guard (see the debug triple)
     DE_DEGEN = 32u,        // a 3D cut met degenerate geometry (a face cut twice, an open new face)
+    DE_SIDE = 64u,         // a long row did not fit the side buffer (the host grows it and runs again)
 };
 
 }  // namespace sdot

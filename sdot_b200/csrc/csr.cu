@@ -107,6 +107,64 @@ __global__ void k_unpermute(const double *in, double *out, long long n, int d, c
     for (int k = 0; k < d; ++k) out[i * d + k] = in[s * d + k];
 }
 
+// ---- domains of several shapes: one cell pass per shape, summed here
+__global__ void k_rows_clear(Rows R, long long n) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s < n) R.cnt[s] = 0;
+}
+
+// dst row s += src row s (entries appended; a row that outgrows the ELL
+// width moves, with the new entries, to a fresh place in the side buffer)
+__global__ void k_rows_append(Rows dst, Rows src, long long n, unsigned *err) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int m0 = dst.cnt[s], m1 = src.cnt[s], m = m0 + m1;
+    if (m1 == 0) return;
+    if (m <= dst.cap) {
+        for (int k = 0; k < m1; ++k) {
+            dst.col[(m0 + k) * dst.stride + s] = *src.colp(s, k);
+            if (dst.val) dst.val[(m0 + k) * dst.stride + s] = *src.valp(s, k);
+        }
+        dst.cnt[s] = m;
+        return;
+    }
+    const unsigned long long off = atomicAdd(dst.side_used, (unsigned long long)m);
+    if ((long long)(off + m) > dst.side_cap) {
+        atomicOr(err, unsigned(DE_SIDE));
+        return;
+    }
+    for (int k = 0; k < m0; ++k) {
+        dst.side_col[off + k] = *dst.colp(s, k);
+        if (dst.side_val) dst.side_val[off + k] = *dst.valp(s, k);
+    }
+    for (int k = 0; k < m1; ++k) {
+        dst.side_col[off + m0 + k] = *src.colp(s, k);
+        if (dst.side_val) dst.side_val[off + m0 + k] = *src.valp(s, k);
+    }
+    dst.side[s] = (long long)off;
+    dst.cnt[s] = m;
+}
+
+// mass += t_mass, mass_c += t_mass_c, mom += t_ctd * t_mass_c (2D)
+__global__ void k_accum2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                         const double *t_ctd, long long n) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    mass[s] += t_mass[s];
+    mass_c[s] += t_mass_c[s];
+    mom[2 * s] += t_ctd[2 * s] * t_mass_c[s];
+    mom[2 * s + 1] += t_ctd[2 * s + 1] * t_mass_c[s];
+}
+
+// centroid = moment / (mass + (mass == 0)), as get_centroids divides
+__global__ void k_ctd_final2(double *ctd, const double *mom, const double *mass_c, long long n) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double d = mass_c[s] + (mass_c[s] == 0);
+    ctd[2 * s] = mom[2 * s] / d;
+    ctd[2 * s + 1] = mom[2 * s + 1] / d;
+}
+
 }  // namespace
 
 void csr_read_checks(unsigned long long out[3]) {
@@ -145,6 +203,32 @@ void nb_write(const Rows &NB, long long n, const int *idx, const long long *offs
 void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st) {
     if (n <= 0) return;
     k_unpermute<<<ceil_div(n, TB), TB, 0, st>>>(in, out, n, d, idx);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+
+void rows_clear(const Rows &R, long long n, cudaStream_t st) {
+    if (n <= 0) return;
+    k_rows_clear<<<ceil_div(n, TB), TB, 0, st>>>(R, n);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+void rows_append(const Rows &dst, const Rows &src, long long n, unsigned *err, cudaStream_t st) {
+    if (n <= 0) return;
+    k_rows_append<<<ceil_div(n, TB), TB, 0, st>>>(dst, src, n, err);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                 const double *t_ctd, long long n, cudaStream_t st) {
+    if (n <= 0) return;
+    k_accum2<<<ceil_div(n, TB), TB, 0, st>>>(mass, mass_c, mom, t_mass, t_mass_c, t_ctd, n);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st) {
+    if (n <= 0) return;
+    k_ctd_final2<<<ceil_div(n, TB), TB, 0, st>>>(ctd, mom, mass_c, n);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }

@@ -19,6 +19,14 @@ void nb_counts(const Rows &NB, long long n, const int *idx, long long *cnt_orig,
 void nb_write(const Rows &NB, long long n, const int *idx, const long long *offsets, long long *ids, cudaStream_t st);
 // First failed debug check of the assembly kernels (zeros in release builds).
 void csr_read_checks(unsigned long long out[3]);
+// Domains of several shapes (one cell pass per shape): empty all rows;
+// append the rows of one pass; sum one pass's masses and centroid moments;
+// divide the moments (get_centroids' mass + (mass == 0)).
+void rows_clear(const Rows &R, long long n, cudaStream_t st);
+void rows_append(const Rows &dst, const Rows &src, long long n, unsigned *err, cudaStream_t st);
+void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                 const double *t_ctd, long long n, cudaStream_t st);
+void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st);
 // out[idx[s] * d + k] = in[s * d + k]
 void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st);
 

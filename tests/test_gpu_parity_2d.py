@@ -129,25 +129,8 @@ def test_image_density_disc_clip(gpu_lib, ref_oracle):
     check_all(gpu, ref, 5000, rtol=1e-11)
 
 
-MULTI_OFF = ("the multi-shape cell kernel raised an illegal address in a release build while a bounds-checked "
-             "build of the same kernel ran clean; it stays disabled until the cause is found")
-
-
-def test_multi_items_rejected(gpu_lib):
-    # the disabled path fails loudly, before any kernel is launched
-    from sdot_b200._lib import SDOT_UNSUPPORTED, SdotError
-    from sdot_b200.power_diagram import PowerDiagram
-
-    g = PowerDiagram(np.random.default_rng(0).random((10, 2)) * [2.0, 1.0], np.zeros(10))
-    g.add_box_shape([0.0, 0.0], [1.0, 1.0], 1.0)
-    g.add_box_shape([1.0, 0.0], [2.0, 1.0], 0.5)
-    with pytest.raises(SdotError) as e:
-        g.integrals()
-    assert e.value.status == SDOT_UNSUPPORTED
-
-
-@pytest.mark.skip(reason=MULTI_OFF)
 def test_multi_items(gpu_lib, ref_oracle):
+    # several shapes with different densities: one cell pass per shape
     rng = np.random.default_rng(5)
     n = 2000
     p = rng.random((n, 2)) * [2.0, 1.0]
@@ -158,7 +141,6 @@ def test_multi_items(gpu_lib, ref_oracle):
     check_all(gpu, ref, n)
 
 
-@pytest.mark.skip(reason=MULTI_OFF)
 def test_multi_items_disc_clip(gpu_lib, ref_oracle):
     rng = np.random.default_rng(8)
     n = 1500

@@ -57,3 +57,14 @@ def test_newton_3d(gpu_lib, ref_oracle):
     assert rep["converged"]
     w_g = gpu.get_weights()
     assert np.abs(w_g - w_r).max() <= 1e-10 * np.abs(w_r).max()
+
+
+def test_clustered_cube(gpu_lib, ref_oracle):
+    # 20 Gaussian clusters (sigma 0.02, mirrored at the faces): cells on the
+    # clusters' rims reach far into the empty space and have many faces (the
+    # larger-capacity passes)
+    rng = np.random.default_rng(34)
+    n = 30000
+    p = workloads.clustered_points(n, 3, rng, boundary="reflect")
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle)
+    check_all(gpu, ref, n, rtol=1e-11, rtol_hess=1e-10)
