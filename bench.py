@@ -1,7 +1,8 @@
 """Benchmark of the power-diagram hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--n DIRACS]
+                    [--precision fp64|mixed] [--n DIRACS] [--config c2|c4]
+    python bench.py --serving [--requests R] [--slots S]
 
 Workload: the 2D power diagram at scale -- 1,000,000 Diracs, 50% uniform in
 [0,1]^2 and 50% from 20 Gaussian clusters (sigma 0.02, clamped to the box),
@@ -9,6 +10,8 @@ weights uniform in [-1e-6, 1e-6], unit box with density 1 (seeded synthetic
 data, sdot_b200/workloads.py).  One step is one fused evaluation: device
 Z-order tree build, every Laguerre cell, cell areas, centroids and the CSR
 weight Hessian.  Metric: Laguerre cells per second (areas + Hessian).
+--config c4 runs the 3D workload instead: 200,000 Diracs (70% uniform, 30% on
+a jittered lattice), w = 0, unit cube, density (1 + 0.3 xyz) normalised.
 
 Arms
   ours       : libsdot_b200.so through its C ABI.  `value` is timed with CUDA
@@ -49,6 +52,12 @@ FLOPS_PER_CELL = 3.9e3
 # per-cell algorithmic HBM bytes: positions + weight in (24), area (8),
 # centroid (16), ~7 Hessian entries x 12 + offset 8
 BYTES_PER_CELL = 136.0
+# 3D (reference counts on the 3D workload): 61.8 cut attempts x (12 + 5 x 25
+# effective vertices) + 81.9 boxes x 20.7 vertices x 12 + 14.9 faces of 25.8
+# vertices integrated ~ 27.5 kflop; bytes: 32 in, 8 volume, 24 centroid,
+# ~16 Hessian entries x 12 + 8 offset
+FLOPS_PER_CELL_3D = 27.5e3
+BYTES_PER_CELL_3D = 264.0
 
 
 def hbm_peak():
@@ -67,7 +76,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--n", type=int, default=0, help="Diracs per GPU (default 1M for c2, 200k for c4)")
+    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
+                    help="c2: 2D 1M clustered mix (the headline); c4: 3D 200k uniform + jittered lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", action="store_true",
                     help="serving benchmark: a Poisson stream of OT solves, continuous batching vs sequential")
@@ -83,9 +94,11 @@ def dist_env():
     return rank, world, local
 
 
-def workload(n, rank):
+def workload(n, rank, config="c2"):
     from sdot_b200 import workloads
 
+    if config == "c4":
+        return workloads.config4(n=n)
     c = workloads.config2(n=n)
     if rank:
         # another seeded problem of the same shape per extra rank
@@ -95,6 +108,16 @@ def workload(n, rank):
                                          workloads.clustered_points(n - nu, 2, rng)])
         c["weights"] = rng.uniform(-1e-6, 1e-6, n)
     return c
+
+
+def describe(config):
+    """(metric, workload description) of a bench configuration."""
+    if config == "c4":
+        return ("Laguerre cells/s (volumes + centroids + CSR Hessian), 3D, 200k Diracs",
+                "3D power diagram, 200k Diracs (70% uniform + 30% jittered lattice), w = 0, unit cube, "
+                "density (1 + 0.3 xyz) / 1.0375 integrated exactly; volumes + centroids + CSR Hessian")
+    return (METRIC, "2D power diagram, 1M Diracs (50% uniform + 50% 20-cluster Gaussian sigma 0.02), "
+                    "w ~ U[-1e-6,1e-6], unit box, density 1; areas + centroids + CSR Hessian")
 
 
 # ------------------------------------------------------------------ clocks
@@ -157,9 +180,10 @@ def cpu_reference_step(pos, w, threads):
     requires).  Returns (seconds, kind)."""
     from oracle import ref
 
+    dim = pos.shape[1]
     if ref.available():
         r = ref.RefPowerDiagram(pos, w, threads=threads)
-        r.add_box_shape([0.0, 0.0], [1.0, 1.0])
+        r.add_box_shape(np.zeros(dim), np.ones(dim))
         t0 = time.perf_counter()
         r.update()
         r.integrals()
@@ -193,7 +217,10 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    c = workload(args.n, 0)
+    c = workload(args.n, 0, args.config)
+    metric, wl = describe(args.config)
+    if args.config == "c4":
+        wl += " (the reference has no smooth 3D density: it runs the same diagram at density 1)"
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_reference_step(c["positions"], c["weights"], threads)
@@ -206,11 +233,10 @@ def run_reference(args):
     t_all = time.perf_counter() - t_all
     ms = 1e3 * sum(times) / len(times)
     value = args.n / (ms * 1e-3)
-    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+    out = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "2D power diagram, 1M Diracs (50% uniform + 50% clustered), w ~ U[-1e-6,1e-6], "
-                                  "unit box", "n_diracs": args.n, "parallelism": "host threads"},
+           "config": {"workload": wl, "n_diracs": args.n, "parallelism": "host threads"},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind,
                             "sample": f"each step one full evaluation of the {args.n}-Dirac workload"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -231,8 +257,10 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     L = _lib.load()
-    c = workload(args.n, rank)
+    c = workload(args.n, rank, args.config)
     n = args.n
+    dim = 3 if args.config == "c4" else 2
+    flops_cell, bytes_cell = (FLOPS_PER_CELL_3D, BYTES_PER_CELL_3D) if dim == 3 else (FLOPS_PER_CELL, BYTES_PER_CELL)
     pos_h = torch.from_numpy(np.ascontiguousarray(c["positions"])).pin_memory()
     w_h = torch.from_numpy(np.ascontiguousarray(c["weights"])).pin_memory()
     pos_d = pos_h.to(dev)
@@ -240,17 +268,20 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     prec = {"fp64": _lib.SDOT_FP64, "mixed": _lib.SDOT_MIXED}[args.precision]
     opt = _lib.SdotOptions(11, ctypes.c_void_p(stream.cuda_stream), local)
-    ctx = L.sdot_create(2, prec, ctypes.byref(opt))
+    ctx = L.sdot_create(dim, prec, ctypes.byref(opt))
     if not ctx:
         raise RuntimeError("sdot_create failed")
-    p0 = np.zeros(2)
-    p1 = np.ones(2)
+    p0 = np.zeros(dim)
+    p1 = np.ones(dim)
 
     def check(st):
         if st != 0:
             raise RuntimeError(L.sdot_last_error(ctx).decode())
 
     check(L.sdot_add_box_shape(ctx, ctypes.c_void_p(p0.ctypes.data), ctypes.c_void_p(p1.ctypes.data), 1.0))
+    if "density" in c:
+        dens = np.ascontiguousarray(c["density"], dtype=np.float64)
+        check(L.sdot_set_polynomial_density(ctx, ctypes.c_void_p(dens.ctypes.data), int(dens.size)))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step_device():
@@ -303,7 +334,7 @@ def run_ours(args):
     off_h = torch.empty(n + 1, dtype=torch.int64).pin_memory()
     mass_h = torch.empty(n, dtype=torch.float64).pin_memory()
     mass2_h = torch.empty(n, dtype=torch.float64).pin_memory()
-    ctd_h = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+    ctd_h = torch.empty(dim * n, dtype=torch.float64).pin_memory()
     cols_h = vals_h = None
     nnz = ctypes.c_int64(0)
 
@@ -339,36 +370,36 @@ def run_ours(args):
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = n * 2 * 8 + n * 8
-    d2h = n * 16 + n * 8 + (n + 1) * 8 + nnz.value * 16 + n * 8
+    h2d = n * dim * 8 + n * 8
+    d2h = n * dim * 8 + n * 8 + (n + 1) * 8 + nnz.value * 16 + n * 8
 
     # ---- roofline of the cell kernel (the dominant kernel)
     peaks = np.zeros(2)
     L.sdot_measure_fma_peaks(ctypes.c_void_p(peaks.ctypes.data))
     cell = float(np.mean(cell_ms))
-    achieved = FLOPS_PER_CELL * n / (cell * 1e-3) / 1e12
+    achieved = flops_cell * n / (cell * 1e-3) / 1e12
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic_cells2d_c2_1M.json")
-    if os.path.exists(prof):
+    if dim == 2 and os.path.exists(prof):
         with open(prof) as f:
             traffic = json.load(f).get("bytes_per_launch")
-    roofline = {"bound": "fp64", "kernel": "k_cells2d (fast tier) + overflow tiers", "achieved": achieved,
+    kern = "k_cells3d (four capacity passes)" if dim == 3 else "k_cells2d (fast tier) + overflow tiers"
+    roofline = {"bound": "fp64", "kernel": kern, "achieved": achieved,
                 "peak": float(peaks[0]), "unit": "TFLOP/s", "frac": achieved / float(peaks[0]) if peaks[0] else None,
-                "traffic": traffic, "algorithmic_bytes_per_launch": BYTES_PER_CELL * n,
-                "flops_per_cell": FLOPS_PER_CELL, "cell_kernel_ms": cell,
+                "traffic": traffic, "algorithmic_bytes_per_launch": bytes_cell * n,
+                "flops_per_cell": flops_cell, "cell_kernel_ms": cell,
                 "peak_source": "FP64 FMA peak measured in this run by sdot_measure_fma_peaks (FMA-only kernel); "
                                "the path uses no tensor cores and its HBM floor is far below the FP64 one",
-                "hbm_view": {"achieved_gbs": BYTES_PER_CELL * n / (cell * 1e-3) / 1e9, "peak_gbs": hbm_peak(),
-                             "frac": BYTES_PER_CELL * n / (cell * 1e-3) / 1e9 / hbm_peak()},
+                "hbm_view": {"achieved_gbs": bytes_cell * n / (cell * 1e-3) / 1e9, "peak_gbs": hbm_peak(),
+                             "frac": bytes_cell * n / (cell * 1e-3) / 1e9 / hbm_peak()},
                 "fp32_peak_tflops": float(peaks[1])}
 
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    metric, wl = describe(args.config)
+    out = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-           "data": "synthetic (seeded, shapes of the 1M-Dirac clustered 2D workload)",
-           "config": {"workload": "2D power diagram, 1M Diracs (50% uniform + 50% 20-cluster Gaussian sigma 0.02), "
-                                  "w ~ U[-1e-6,1e-6], unit box, density 1; areas + centroids + CSR Hessian",
-                      "n_diracs_per_gpu": n, "precision": args.precision,
+           "data": "synthetic (seeded, shapes of the named workload)",
+           "config": {"workload": wl, "n_diracs_per_gpu": n, "precision": args.precision,
                       "parallelism": f"weak x{world} (independent problem per GPU)",
                       "l2": "flushed between steps (256 MB write)"},
            "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -377,7 +408,7 @@ def run_ours(args):
            "stages_ms": {"cells": cell}}
     # ---- outside the timed region: the mixed-precision path on the same
     # problem (cells/s and its error against the FP64 path) and Newton times
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and dim == 2:
         try:
             out["mixed"] = mixed_leg(L, c, n, dev, flush, args.steps)
         except Exception as e:  # reported, never required
@@ -389,6 +420,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(c)
+            if dim == 3:
+                out["cpu_baseline"]["sample"] += " (at density 1: the reference has no smooth 3D density)"
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)}
     L.sdot_destroy(ctx)
@@ -467,7 +500,7 @@ def run_stream(reqs, slots, rate_scale, tol):
         ids.append(srv.submit(r["positions"], np.full(r["n"], 1.0 / r["n"])))
     srv.drain()
     wall = time.perf_counter() - t0
-    reps = [srv.result(i)[1] for i in ids]
+    reps = [srv.poll(i)[2] for i in ids]  # failed requests are counted, not raised
     srv.close()
     lat = np.array([(rp["end_ms"] - rp["submit_ms"]) * 1e-3 for rp in reps])
     return lat, reps, wall
@@ -504,6 +537,8 @@ def run_serving(args):
 
 def main():
     args = parse()
+    if not args.n:
+        args.n = 200_000 if args.config == "c4" else 1_000_000
     if args.serving:
         run_serving(args)
     elif args.impl == "reference":

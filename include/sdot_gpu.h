@@ -81,6 +81,15 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
 int sdot_add_simplex_shape(sdot_ctx *ctx, const double *points, double coeff);
 int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const double *data,
                            const int64_t *sizes, int nb_coeffs);
+/* Multilinear density factor (3D): the domain's density becomes
+ *   coeff * (c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz)
+ * in absolute coordinates (nb_coeffs = 8; nb_coeffs = 1 restores a constant
+ * factor).  No reference counterpart: the reference's 3D densities are
+ * piecewise constant (ScaledImage with nb_coeffs = 1, Polynomial.h:53-58);
+ * this one integrates exactly the smooth density 1 + 0.3 xyz of the 3D
+ * benchmark workload.  Cleared by sdot_clear_domain; counted by
+ * sdot_domain_measure and sdot_normalize_domain.  2D: SDOT_UNSUPPORTED.     */
+int sdot_set_polynomial_density(sdot_ctx *ctx, const double *coeffs, int nb_coeffs);
 int sdot_clear_domain(sdot_ctx *ctx);
 int sdot_normalize_domain(sdot_ctx *ctx);
 int sdot_domain_measure(sdot_ctx *ctx, double *measure);

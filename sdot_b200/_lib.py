@@ -81,6 +81,7 @@ SIGNATURES = {
     "sdot_add_convex_polyhedron_shape": (ctypes.c_int, [_P, _P, _P, _I64, ctypes.c_double]),
     "sdot_add_simplex_shape": (ctypes.c_int, [_P, _P, ctypes.c_double]),
     "sdot_set_image_density": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
+    "sdot_set_polynomial_density": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "sdot_clear_domain": (ctypes.c_int, [_P]),
     "sdot_normalize_domain": (ctypes.c_int, [_P]),
     "sdot_domain_measure": (ctypes.c_int, [_P, _P]),

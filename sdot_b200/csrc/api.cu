@@ -108,6 +108,8 @@ struct sdot_ctx {
         double lo[3], hi[3], coeff;
     };
     std::vector<Box3> boxes3;  // 3D domain: boxes (one supported)
+    bool has_poly = false;     // 3D multilinear density factor
+    double poly3[8] = {1, 0, 0, 0, 0, 0, 0, 0};
     bool has_image = false;
     double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};
     long long img_size[2] = {0, 0};
@@ -378,6 +380,8 @@ struct sdot_ctx {
             a.box_hi[d] = boxes3[0].hi[d];
         }
         a.coeff = boxes3[0].coeff;
+        a.has_poly = has_poly ? 1 : 0;
+        for (int k = 0; k < 8; ++k) a.poly[k] = poly3[k];
         a.ovf_list = ovf_list;
         a.ovf_cnt = ovf_cnt;
         a.ovf_list2 = ovf_list2;
@@ -478,7 +482,7 @@ struct sdot_ctx {
             return SDOT_ITER_CAP;
         }
         if (last_err & DE_CAPACITY) {
-            last_error = dim == 3 ? "a cell exceeded the maximum polyhedron capacity (128 faces of 64 vertices)"
+            last_error = dim == 3 ? "a cell exceeded the maximum polyhedron capacity (256 faces of 128 vertices)"
                                   : "a cell exceeded the maximum polygon capacity (1024 vertices)";
             return SDOT_CAPACITY;
         }
@@ -644,6 +648,12 @@ struct sdot_ctx {
                 set_device_weights_changed();
                 st = evaluate();
                 ++rep.evaluations;
+                if (st == SDOT_CAPACITY && o.damping) {
+                    // a trial step so long that a cell outgrew the kernels'
+                    // polyhedra is rejected like one that raised the error
+                    tau *= 0.5;
+                    continue;
+                }
                 if (st != SDOT_OK) return st;
                 mass_stats(s_mass, en);
                 if (!o.damping || en[0] <= o.rel_mass_tol ||
@@ -654,9 +664,13 @@ struct sdot_ctx {
                 tau *= 0.5;
             }
             if (!accepted) {
-                // no acceptable step: keep the last accepted weights
+                // no acceptable step: keep the last accepted weights (and
+                // their cells, so that the outputs match the weights)
                 SDOT_CUDA(cudaMemcpyAsync(d_w, w_old, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
                 set_device_weights_changed();
+                st = evaluate();
+                ++rep.evaluations;
+                if (st != SDOT_OK) return st;
                 char buf[160];
                 snprintf(buf, sizeof buf,
                          "damped Newton: no step length decreased the mass error (max relative mass error %.3e)", e[0]);
@@ -917,10 +931,27 @@ int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *ma
     });
 }
 
+int sdot_set_polynomial_density(sdot_ctx *ctx, const double *coeffs, int nb_coeffs) {
+    return guarded(ctx, [&] {
+        if (!coeffs) throw BadArg("null coefficients");
+        if (ctx->dim != 3) throw Unsupported("polynomial densities are available in 3D only");
+        if (nb_coeffs != 1 && nb_coeffs != 8) throw BadArg("nb_coeffs must be 1 or 8");
+        for (int k = 0; k < nb_coeffs; ++k)
+            if (!std::isfinite(coeffs[k])) throw BadArg("non-finite density coefficient");
+        for (int k = 0; k < 8; ++k) ctx->poly3[k] = k < nb_coeffs ? coeffs[k] : 0.0;
+        ctx->has_poly = nb_coeffs == 8;
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
+        return int(SDOT_OK);
+    });
+}
+
 int sdot_clear_domain(sdot_ctx *ctx) {
     return guarded(ctx, [&] {
         ctx->items.clear();
         ctx->boxes3.clear();
+        ctx->has_poly = false;
+        for (int k = 0; k < 8; ++k) ctx->poly3[k] = k == 0 ? 1.0 : 0.0;
         ctx->has_image = false;
         ctx->dom_dirty = true;
         ctx->mark_dirty();
@@ -939,8 +970,19 @@ static double domain_measure(const sdot_ctx *ctx) {
     }
     double res = 0;
     for (const Item2 &it : ctx->items) res += it.coeff * it.area();
-    for (const sdot_ctx::Box3 &b : ctx->boxes3)
-        res += b.coeff * (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
+    for (const sdot_ctx::Box3 &b : ctx->boxes3) {
+        // integral over the box of the multilinear factor: per monomial, a
+        // product over the axes of (hi - lo) or (hi^2 - lo^2) / 2
+        static const int axes[8] = {0, 1, 2, 4, 3, 5, 6, 7};  // bit d: u_d in the monomial
+        double f = 0;
+        for (int k = 0; k < 8; ++k) {
+            double t = ctx->poly3[k];
+            for (int d = 0; d < 3; ++d)
+                t *= (axes[k] >> d & 1) ? 0.5 * (b.hi[d] * b.hi[d] - b.lo[d] * b.lo[d]) : b.hi[d] - b.lo[d];
+            f += t;
+        }
+        res += b.coeff * f;
+    }
     return res;
 }
 

@@ -222,31 +222,47 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
         cell.Y(k) = A.start_xy[2 * k + 1];
         cell.I(k) = domain_id(k);
     }
+    // The walk's memory reads are issued a step before their use, so that
+    // their latency overlaps the vertex pass of the step before: the node
+    // popped next is kept in a register (the stack holds the others), and the
+    // position and weight of the next Dirac of a leaf are loaded while the
+    // current one cuts.
     int stack[STACK];
-    int sp = 0;
-    stack[sp++] = 0;
-    int j = 0, je = 0;  // Diracs of the current leaf still to cut by
+    int sp = 0;                 // stack entries below `top`
+    int top = 0;                // the node the next node step pops
+    bool has_top = true;
+    int j = 0, je = 0;          // Diracs of the current leaf still to cut by
+    double cjx = 0, cjy = 0, cjw = 0;  // Dirac j
     int visits = 0;
+    auto skip_self = [&](int k) { return k == s ? k + 1 : k; };
     while (true) {
         // ---- the step: one cut (j < je) or one node test
         const bool is_cut = j < je;
         double ox = 0, oy = 0, nx = 0, ny = 0;
         double lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0, maxw = 0;
         int node = -1, nd_a = 0, nd_b = 0;
+        int jn = 0;
+        double njx = 0, njy = 0, njw = 0;
         if (is_cut) {
-            if (j == s) {
-                ++j;
-                continue;
+            bisector(c0x, c0y, w0, cjx, cjy, cjw, ox, oy, nx, ny);
+            jn = skip_self(j + 1);
+            if (jn < je) {
+                (void)SDOT_CHECK_IDX(jn, A.n, 6);
+                njx = A.pos[2 * jn];
+                njy = A.pos[2 * jn + 1];
+                njw = A.w[jn];
             }
-            (void)SDOT_CHECK_IDX(j, A.n, 6);
-            bisector(c0x, c0y, w0, A.pos[2 * j], A.pos[2 * j + 1], A.w[j], ox, oy, nx, ny);
         } else {
-            if (sp == 0) break;
+            if (!has_top) break;
             if (++visits > A.max_nodes) {  // a tree visits each node once: a cycle means a corrupt tree
                 flag_error(A.err, DE_ITER);
                 return -1;
             }
-            node = stack[--sp];
+            node = top;
+            if (sp > 0)
+                top = stack[--sp];
+            else
+                has_top = false;
             const TreeNode<2> &nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
             lo0 = nd.lo[0];
             lo1 = nd.lo[1];
@@ -273,7 +289,10 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
                 if (n <= 0) return n;
             }
-            ++j;
+            j = jn;
+            cjx = njx;
+            cjy = njy;
+            cjw = njw;
             continue;
         }
         if (f.nb_out == 0) continue;  // every vertex passes: the box is evicted
@@ -308,14 +327,23 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 key[q + 1] = kk;
                 ch[q + 1] = cc;
             }
-            for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
+            for (int c = 0; c < nch; ++c) {
+                if (has_top) stack[sp++] = top;
+                top = ch[c];
+                has_top = true;
+            }
         } else {
             if (nd_a < 0 || nd_b > A.n) {
                 guard_fail(A, 2, s, node);
                 return -2;
             }
-            j = nd_a;
+            j = skip_self(nd_a);
             je = nd_b;
+            if (j < je) {
+                cjx = A.pos[2 * j];
+                cjy = A.pos[2 * j + 1];
+                cjw = A.w[j];
+            }
         }
     }
     return n;

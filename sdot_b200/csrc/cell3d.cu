@@ -1,7 +1,7 @@
 // 3D Laguerre-cell kernels (see cell3d.cuh).
 //
 // One warp builds one cell.  The cell is a convex polyhedron held as its
-// faces, one face per lane (two in the large pass): each face is a polygon
+// faces, one face per lane (2, 4 or 8 in the larger passes): each face is a polygon
 // (vertices counter-clockwise seen from outside, in coordinates relative to
 // the cell's Dirac) whose edge k carries the id of the face across it, plus
 // the face's plane a . u <= b and its cut id (a Dirac index, or a domain
@@ -23,9 +23,17 @@
 //  * face area by a fan of triangles (ConvexPolyhedron3::area, :1367-1419);
 //  * Hessian row: -1/2 coeff area / |x_i - x_j| per neighbour face, the
 //    diagonal their sum; domain faces skipped (get_der_integrals_wrt_weights.h:43-88).
+//
+// Multilinear density (an extension: the reference's 3D densities are
+// piecewise constant).  Relative to the cell's Dirac the density is
+// sum_k g_k(u), g_k homogeneous of degree k <= 3, and by Euler's identity
+// div(u g_k) = (k + 3) g_k, so the pyramid of a face at signed distance h
+// holds h/(k+3) times the face integral of g_k (and u g_k, of degree k + 1,
+// h/(k+4) times its face integral).  The face integrals use Dunavant's
+// degree-4 rule on each fan triangle (6 points; D. A. Dunavant, "High degree
+// efficient symmetrical Gaussian quadrature rules for the triangle", IJNME
+// 21, 1985), exact for every term here.
 #include "cell3d.cuh"
-
-#include <type_traits>
 
 namespace sdot {
 
@@ -61,31 +69,23 @@ struct Cell3 {
 __device__ inline double shfl(double v, int src) { return __shfl_sync(FULL, v, src); }
 
 // Outcome of a cut: 0 done, 1 a capacity was exceeded, 2 degenerate geometry.
-// bit masks over the vertices of one face
-__device__ inline int popc_m(unsigned m) { return __popc(m); }
-__device__ inline int popc_m(unsigned long long m) { return __popcll(m); }
-__device__ inline int ffs_m(unsigned m) { return __ffs(int(m)); }
-__device__ inline int ffs_m(unsigned long long m) { return __ffsll((long long)m); }
-
 template <int FPL, int MAXV>
 __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double qb, int qid) {
-    using Mask = typename std::conditional<(MAXV > 32), unsigned long long, unsigned>::type;
-    constexpr int MB = 8 * sizeof(Mask);
     const int lane = threadIdx.x & 31;
     auto &F = C.F;
-    Mask mask[FPL];
+    auto outside = [&](int v, int f) {
+        const int i = F.at(v, f);
+        return qb - (qx * F.X[i] + qy * F.Y[i] + qz * F.Z[i]) < 0.0;
+    };
+    int nouts[FPL];
     bool has = false;
 #pragma unroll
     for (int r = 0; r < FPL; ++r) {
         const int f = lane + 32 * r;
-        Mask m = 0;
-        for (int v = 0; v < C.nv[r]; ++v) {
-            const int i = F.at(v, f);
-            const double d = qb - (qx * F.X[i] + qy * F.Y[i] + qz * F.Z[i]);
-            m |= Mask(d < 0.0) << v;
-        }
-        mask[r] = m;
-        has |= m != 0;
+        int c = 0;
+        for (int v = 0; v < C.nv[r]; ++v) c += outside(v, f);
+        nouts[r] = c;
+        has |= c != 0;
     }
     if (!__any_sync(FULL, has)) return 0;
     // ---- cut every face
@@ -100,24 +100,29 @@ __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double
         exit_nb[r] = 0;
         ex[r] = ey[r] = ez[r] = 0;
         const int n = C.nv[r];
-        if (n == 0 || mask[r] == 0) continue;
-        const Mask full = n >= MB ? ~Mask(0) : ((Mask(1) << n) - 1);
-        const Mask outs = mask[r] & full;
-        if (outs == full) {  // the whole face is removed
+        const int nout = nouts[r];
+        if (n == 0 || nout == 0) continue;
+        if (nout == n) {  // the whole face is removed
             C.nv[r] = 0;
             continue;
         }
-        // out vertex k whose predecessor is in: the start of the outside run
-        const Mask prev_out = ((outs << 1) | (outs >> (n - 1))) & full;  // bit k: vertex k - 1 is out
-        const Mask starts = outs & ~prev_out;
-        const Mask next_out = ((outs >> 1) | (outs << (n - 1))) & full;  // bit k: vertex k + 1 is out
-        const Mask ends = outs & ~next_out;
-        if (popc_m(starts) != 1 || popc_m(ends) != 1) {
+        // the outside run: o1 its first vertex (predecessor inside), o2 its
+        // last (successor inside); one run only, else the face is cut twice
+        int o1 = -1, o2 = -1, runs = 0;
+        bool prev = outside(n - 1, f);
+        for (int v = 0; v < n; ++v) {
+            const bool o = outside(v, f);
+            if (o && !prev) {
+                o1 = v;
+                ++runs;
+            }
+            if (!o && prev) o2 = v == 0 ? n - 1 : v - 1;
+            prev = o;
+        }
+        if (runs != 1 || o1 < 0 || o2 < 0) {
             bad = true;
             continue;
         }
-        const int o1 = ffs_m(starts) - 1, o2 = ffs_m(ends) - 1;
-        const int nout = popc_m(outs);
         const int il = o1 == 0 ? n - 1 : o1 - 1;  // last inside vertex before the run
         const int fi = o2 == n - 1 ? 0 : o2 + 1;  // first inside vertex after it
         const int nn = n - nout + 2;
@@ -242,6 +247,53 @@ __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double
     __syncwarp();
     return 0;
 }
+
+// A multilinear density rewritten about the cell's Dirac c: coefficients of
+// 1, u_x, u_y, u_z, u_x u_y, u_x u_z, u_y u_z, u_x u_y u_z for u = x - c.
+struct PolyRel {
+    double b1, bx, by, bz, bxy, bxz, byz, bxyz;
+    __device__ PolyRel(const double *a, double cx, double cy, double cz) {
+        bxyz = a[7];
+        bxy = a[4] + a[7] * cz;
+        bxz = a[5] + a[7] * cy;
+        byz = a[6] + a[7] * cx;
+        bx = a[1] + a[4] * cy + a[5] * cz + a[7] * cy * cz;
+        by = a[2] + a[4] * cx + a[6] * cz + a[7] * cx * cz;
+        bz = a[3] + a[5] * cx + a[6] * cy + a[7] * cx * cy;
+        b1 = a[0] + a[1] * cx + a[2] * cy + a[3] * cz + a[4] * cx * cy + a[5] * cx * cz + a[6] * cy * cz +
+             a[7] * cx * cy * cz;
+    }
+    // One point q (relative coordinates) of a face rule with weight wt:
+    // pm += wt * sum_k g_k(q)/(k+3), pd += wt * q * sum_k g_k(q)/(k+4),
+    // pf += wt * sum_k g_k(q).
+    __device__ void add(double qx, double qy, double qz, double wt, double &pm, double &pdx, double &pdy, double &pdz,
+                        double &pf) const {
+        const double g0 = b1;
+        const double g1 = bx * qx + by * qy + bz * qz;
+        const double g2 = bxy * qx * qy + bxz * qx * qz + byz * qy * qz;
+        const double g3 = bxyz * qx * qy * qz;
+        pm += wt * (g0 * (1.0 / 3) + g1 * 0.25 + g2 * 0.2 + g3 * (1.0 / 6));
+        const double gd = wt * (g0 * 0.25 + g1 * 0.2 + g2 * (1.0 / 6) + g3 * (1.0 / 7));
+        pdx += gd * qx;
+        pdy += gd * qy;
+        pdz += gd * qz;
+        pf += wt * (g0 + g1 + g2 + g3);
+    }
+    // Dunavant's degree-4 rule on the triangle p0, p0 + e1, p0 + e2 of area ta.
+    __device__ void triangle(double x0, double y0, double z0, double e1x, double e1y, double e1z, double e2x,
+                             double e2y, double e2z, double ta, double &pm, double &pdx, double &pdy, double &pdz,
+                             double &pf) const {
+        constexpr double A[2] = {0.4459484909159648863, 0.0915762135097707435};
+        constexpr double W[2] = {0.2233815896780114657, 0.1099517436553218676};
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+            const double a = A[g], b = 1.0 - 2.0 * A[g], wt = W[g] * ta;
+            add(x0 + a * (e1x + e2x), y0 + a * (e1y + e2y), z0 + a * (e1z + e2z), wt, pm, pdx, pdy, pdz, pf);
+            add(x0 + b * e1x + a * e2x, y0 + b * e1y + a * e2y, z0 + b * e1z + a * e2z, wt, pm, pdx, pdy, pdz, pf);
+            add(x0 + a * e1x + b * e2x, y0 + a * e1y + b * e2y, z0 + a * e1z + b * e2z, wt, pm, pdx, pdy, pdz, pf);
+        }
+    }
+};
 
 // The domain box as six faces (slots 0..5), relative to c0.
 template <int FPL, int MAXV>
@@ -432,6 +484,8 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
     double rval[FPL];
     bool rmine[FPL], nmine[FPL];
     if (status == 0) {
+        const bool poly = A.has_poly;
+        const PolyRel pr(A.poly, c0x, c0y, c0z);
 #pragma unroll
         for (int r = 0; r < FPL; ++r) {
             const int f = lane + 32 * r;
@@ -445,26 +499,39 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
             const int i0 = C.F.at(0, f);
             const double x0 = C.F.X[i0], y0 = C.F.Y[i0], z0 = C.F.Z[i0];
             double area = 0, fx = 0, fy = 0, fz = 0;
+            double pm = 0, pdx = 0, pdy = 0, pdz = 0, pf = 0;  // density-weighted (poly)
             for (int k = 1; k + 1 < n; ++k) {
                 const int i1 = C.F.at(k, f), i2 = C.F.at(k + 1, f);
                 const double e1x = C.F.X[i1] - x0, e1y = C.F.Y[i1] - y0, e1z = C.F.Z[i1] - z0;
                 const double e2x = C.F.X[i2] - x0, e2y = C.F.Y[i2] - y0, e2z = C.F.Z[i2] - z0;
                 const double ta = 0.5 * ((e1y * e2z - e1z * e2y) * ux + (e1z * e2x - e1x * e2z) * uy +
                                          (e1x * e2y - e1y * e2x) * uz);
-                area += ta;
-                fx += ta * (3 * x0 + e1x + e2x);
-                fy += ta * (3 * y0 + e1y + e2y);
-                fz += ta * (3 * z0 + e1z + e2z);
+                if (poly) {
+                    pr.triangle(x0, y0, z0, e1x, e1y, e1z, e2x, e2y, e2z, ta, pm, pdx, pdy, pdz, pf);
+                } else {
+                    area += ta;
+                    fx += ta * (3 * x0 + e1x + e2x);
+                    fy += ta * (3 * y0 + e1y + e2y);
+                    fz += ta * (3 * z0 + e1z + e2z);
+                }
             }
             const double h = C.b[r] / na;  // signed distance of the face plane from c0
-            const double v = h * area / 3;
-            vol += v;
-            // pyramid centroid: 3/4 of the way from the apex to the face centroid
-            if (area != 0) {
-                const double k = v * 0.75 / (3 * area);
-                mx += k * fx;
-                my += k * fy;
-                mz += k * fz;
+            if (poly) {
+                vol += h * pm;
+                mx += h * pdx;
+                my += h * pdy;
+                mz += h * pdz;
+                area = pf;  // the face's density integral
+            } else {
+                const double v = h * area / 3;
+                vol += v;
+                // pyramid centroid: 3/4 of the way from the apex to the face centroid
+                if (area != 0) {
+                    const double k = v * 0.75 / (3 * area);
+                    mx += k * fx;
+                    my += k * fy;
+                    mz += k * fz;
+                }
             }
             if (C.fid[r] >= 0) {
                 const double bd = 0.5 * A.coeff * area / na;  // |x_i - x_j| = |a|
@@ -582,11 +649,15 @@ void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *nex
     SDOT_CUDA(cudaGetLastError());
 }
 
-constexpr long long G3_WARPS = 148;  // warps of the global-memory pass
+constexpr long long G3_WARPS = 148;  // warps of the third pass (global memory)
 
 }  // namespace
 
-size_t cells3d_scratch_bytes() { return warp_smem_bytes<4, 64>() * G3_WARPS + 256; }
+constexpr long long G4_WARPS = 32;  // warps of the largest pass
+size_t cells3d_scratch_bytes() {
+    const size_t a = warp_smem_bytes<4, 64>() * G3_WARPS, b = warp_smem_bytes<8, 128>() * G4_WARPS;
+    return (a > b ? a : b) + 256;
+}
 
 void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st) {
     if (a.n == 0) return;
@@ -598,8 +669,13 @@ void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st) {
     // the larger passes take the overflow lists (their lengths are on the
     // device: every warp of the launch reads them)
     launch3<2, 32, 1>(a, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2, 148LL * 3, nullptr, 148LL * 3, st);
-    launch3<4, 64, 1>(a, a.ovf_list2, a.ovf_cnt2, nullptr, nullptr, G3_WARPS, static_cast<char *>(scratch), G3_WARPS,
+    // pass 3 hands its overflow to pass 4 through the first list (pass 2
+    // has consumed it); passes 3 and 4 share the scratch, one after the other
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+    launch3<4, 64, 1>(a, a.ovf_list2, a.ovf_cnt2, a.ovf_list, a.ovf_cnt, G3_WARPS, static_cast<char *>(scratch), G3_WARPS,
                       st);
+    launch3<8, 128, 1>(a, a.ovf_list, a.ovf_cnt, nullptr, nullptr, G4_WARPS, static_cast<char *>(scratch), G4_WARPS,
+                       st);
 }
 
 }  // namespace sdot

@@ -20,6 +20,10 @@ struct Cell3DArgs {
     int max_nodes = 1 << 30;
     double box_lo[3] = {0, 0, 0}, box_hi[3] = {1, 1, 1};  // the domain (one box)
     double coeff = 1.0;                                    // its density
+    // optional multilinear density factor (has_poly): coeff * (p0 + p1 x +
+    // p2 y + p3 z + p4 xy + p5 xz + p6 yz + p7 xyz), absolute coordinates
+    int has_poly = 0;
+    double poly[8] = {1, 0, 0, 0, 0, 0, 0, 0};
     double *mass = nullptr;  // n
     double *ctd = nullptr;   // 3n
     Rows rows;               // Hessian rows (rows.cnt null: skipped)
@@ -34,8 +38,8 @@ struct Cell3DArgs {
 
 // First pass over every cell (up to 32 faces of 16 vertices, shared memory),
 // then the cells that overflowed it (64 faces of 32 vertices, shared memory),
-// then those that overflowed again (128 faces of 64 vertices, in `scratch`
-// of cells3d_scratch_bytes() bytes).
+// then those that overflowed again (128 faces of 64 vertices, then 256 faces
+// of 128 vertices, both in `scratch` of cells3d_scratch_bytes() bytes).
 size_t cells3d_scratch_bytes();
 void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st);
 

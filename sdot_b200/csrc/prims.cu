@@ -216,11 +216,9 @@ void radix_sort_pairs(const unsigned *keys_in, const unsigned *vals_in, unsigned
     // ping-pong so that the final pass lands in (keys_out, vals_out)
     const unsigned *src_k = keys_in, *src_v = vals_in;
     for (int p = 0; p < passes; ++p) {
-        bool last = p == passes - 1;
-        bool to_out = ((passes - 1 - p) % 2) == 0;
+        const bool to_out = ((passes - 1 - p) % 2) == 0;
         unsigned *dk = to_out ? keys_out : keys_alt;
         unsigned *dv = to_out ? vals_out : vals_alt;
-        (void)last;
         k_radix_hist<<<nb, RADIX_THREADS, 0, st>>>(src_k, n, 8 * p, ghist, nb);
         note_launch();
         SDOT_CUDA(cudaGetLastError());

@@ -117,6 +117,13 @@ class PowerDiagram:
         mx = _f64(max_pt if max_pt is not None else np.ones(self.dim))
         self._check(self._lib.sdot_set_image_density(self._ctx, _ptr(mn), _ptr(mx), _ptr(img), _ptr(sizes), 1))
 
+    def set_polynomial_density(self, coeffs):
+        """3D: multiplies the domain's density by c0 + c1 x + c2 y + c3 z +
+        c4 xy + c5 xz + c6 yz + c7 xyz (8 coefficients; 1 coefficient
+        restores a constant factor).  Integrated exactly."""
+        c = _f64(coeffs).reshape(-1)
+        self._check(self._lib.sdot_set_polynomial_density(self._ctx, _ptr(c), int(c.size)))
+
     def clear_domain(self):
         self._check(self._lib.sdot_clear_domain(self._ctx))
 

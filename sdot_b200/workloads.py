@@ -78,7 +78,13 @@ def config4(n=200_000):
     L = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:nl]
     L = L + rng.uniform(-0.1 / m, 0.1 / m, L.shape)
     p = np.concatenate([uniform_points(nu, 3, rng), L])
-    return {"positions": p, "weights": np.zeros(n), "domain": "unit_cube", "target": np.full(n, 1.0 / n)}
+    return {"positions": p, "weights": np.zeros(n), "domain": "unit_cube", "target": np.full(n, 1.0 / n),
+            "density": C4_DENSITY}
+
+
+# 1 + 0.3 xyz in the multilinear basis (1, x, y, z, xy, xz, yz, xyz),
+# normalised to unit mass on the unit cube (its integral there is 1 + 0.3/8)
+C4_DENSITY = np.array([1.0, 0, 0, 0, 0, 0, 0, 0.3]) / (1.0 + 0.3 / 8)
 
 
 def serving_requests(count=2000, rate_hz=50.0, seed_salt=0):

@@ -68,3 +68,62 @@ def test_clustered_cube(gpu_lib, ref_oracle):
     p = workloads.clustered_points(n, 3, rng, boundary="reflect")
     gpu, ref = make_pair(p, np.zeros(n), ref_oracle)
     check_all(gpu, ref, n, rtol=1e-11, rtol_hess=1e-10)
+
+
+# ---- multilinear density (no reference integrator: the oracle is the qhull
+# restatement in oracle/poly3d.py, pinned to the reference at density 1)
+def _dict_rows(off, col, val):
+    H = {}
+    for i in range(len(off) - 1):
+        for k in range(off[i], off[i + 1]):
+            H[(i, int(col[k]))] = H.get((i, int(col[k])), 0.0) + val[k]
+    return H
+
+
+@pytest.mark.parametrize("coeffs", ["c4", "random"])
+def test_polynomial_density_vs_oracle(gpu_lib, coeffs):
+    from oracle import poly3d
+    from sdot_b200.power_diagram import PowerDiagram
+
+    rng = np.random.default_rng(41)
+    n = 400
+    p = rng.random((n, 3))
+    w = rng.uniform(-1, 1, n) * 0.2 * (1.0 / n) ** (2 / 3)
+    if coeffs == "c4":
+        a = workloads.C4_DENSITY
+    else:
+        a = np.concatenate([[1.0], rng.uniform(-0.2, 0.2, 7)])
+    g = PowerDiagram(p, w)
+    g.add_box_shape(np.zeros(3), np.ones(3), coeff=1.7)
+    g.set_polynomial_density(a)
+    m_o, c_o, H_o = poly3d.integrate(p, w, poly=a, coeff=1.7)
+    m = g.integrals()
+    c = g.centroids()
+    off, col, val, _ = g.der_integrals_wrt_weights()
+    H = _dict_rows(off, col, val)
+    np.testing.assert_allclose(m, m_o, rtol=1e-11, atol=1e-12 * m_o.mean())
+    np.testing.assert_allclose(c, c_o, rtol=1e-11, atol=1e-12)
+    scale = max(abs(v) for v in H_o.values())
+    keys = set(H) | set(H_o)
+    worst = max(abs(H.get(k, 0.0) - H_o.get(k, 0.0)) for k in keys)
+    assert worst < 1e-11 * scale, worst
+    assert abs(m.sum() - 1.7 * poly3d.box_integral(a)) < 1e-12 * m.sum()
+    assert abs(g.domain_measure() - 1.7 * poly3d.box_integral(a)) < 1e-14
+
+
+def test_config4_density_newton(gpu_lib):
+    # the 3D workload as specified: 200k Diracs, density (1 + 0.3 xyz)
+    # normalised, Newton to a relative mass error of 1e-8 from w = 0
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config4()
+    g = PowerDiagram(c["positions"], c["weights"])
+    g.add_box_shape(np.zeros(3), np.ones(3))
+    g.set_polynomial_density(c["density"])
+    assert abs(g.domain_measure() - 1.0) < 1e-14
+    m0 = g.integrals()
+    assert abs(m0.sum() - 1.0) < 1e-12
+    rep = g.solve_weights(c["target"], rel_mass_tol=1e-8)
+    m = g.integrals()
+    assert np.max(np.abs(m - c["target"]) / c["target"]) <= 1e-8
+    assert rep["iterations"] <= 20
