@@ -129,13 +129,18 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
  * EigenSolver::solve (EigenSolver.cpp:9-41).  Each iteration evaluates the
  * masses and the CSR Hessian on the device, applies the reference's gauge fix
  * (the Hessian entry (0,0) doubled when there is no ball cut, .tcc:62-63),
- * solves H dw = m - target by Jacobi-preconditioned conjugate gradients on
- * the device and sets w -= tau dw.
+ * solves H dw = m - target by preconditioned conjugate gradients on the
+ * device and sets w -= tau dw.  The preconditioner is a multilevel V-cycle
+ * over aggregates of 8 consecutive cells in Morton order (damped Jacobi
+ * smoothing, exact coarsest solve) or plain Jacobi.
  *   damping = 0: the reference rule: tau = 1; when a cell is empty the step
  *                is undone as w = 0.9 w_old + 0.1 w (.tcc:72-79).
  *   damping = 1: Kitagawa-Merigot-Thibert damping: tau halves until every
  *                cell keeps at least half of min(min target, min starting
- *                mass) and |m - target| drops by the factor (1 - tau / 2).
+ *                mass) and |m - target| drops by the factor (1 - tau / 2);
+ *                a trial step whose cells overflow the kernels' capacity is
+ *                rejected like one that fails these tests, and each search
+ *                starts from min(1, 4 x the last accepted tau).
  * Stops when max_i |m_i - target_i| / target_i <= rel_mass_tol (the
  * reference stops on max |dw| < 1e-6, .tcc:111-112).  The solved weights
  * stay in the context (sdot_get_weights).                                    */
@@ -146,6 +151,7 @@ typedef struct sdot_newton_opts {
     double pcg_rel_tol;    /* |H dw - b| <= pcg_rel_tol |b| */
     int damping;           /* 0: reference rule, 1: KMT step halving */
     int verbosity;         /* > 0: one line per Newton iteration on stderr */
+    int preconditioner;    /* 0: multilevel (default), 1: Jacobi */
 } sdot_newton_opts;
 
 typedef struct sdot_newton_report {
@@ -155,10 +161,11 @@ typedef struct sdot_newton_report {
     double min_mass;           /* smallest cell mass at the returned weights */
     double time_ms;            /* wall time of the solve */
     int evaluations;           /* fused cell evaluations done */
+    int pcg_levels;            /* multilevel levels of the last solve (0: Jacobi) */
 } sdot_newton_report;
 
 /* target: double[n] masses (mem_space says where).  opts may be NULL for the
- * defaults {150, 1e-10, 20000, 1e-12, 1, 0}; report may be NULL.
+ * defaults {150, 1e-10, 20000, 1e-12, 1, 0, 0}; report may be NULL.
  * Returns SDOT_OK, SDOT_NOT_CONVERGED (iteration or step-halving cap),
  * SDOT_VOID_CELL (damping = 1 and a cell is empty at the start weights) or
  * an evaluation error.                                                        */

@@ -42,6 +42,7 @@ class SdotNewtonOptions(ctypes.Structure):
         ("pcg_rel_tol", ctypes.c_double),
         ("damping", ctypes.c_int),
         ("verbosity", ctypes.c_int),
+        ("preconditioner", ctypes.c_int),
     ]
 
 
@@ -53,6 +54,7 @@ class SdotNewtonReport(ctypes.Structure):
         ("min_mass", ctypes.c_double),
         ("time_ms", ctypes.c_double),
         ("evaluations", ctypes.c_int),
+        ("pcg_levels", ctypes.c_int),
     ]
 
 

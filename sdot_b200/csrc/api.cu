@@ -454,8 +454,9 @@ struct sdot_ctx {
         SDOT_CUDA(cudaEventElapsedTime(&times[0], ev[0], ev[1]));
         SDOT_CUDA(cudaEventElapsedTime(&times[1], ev[1], ev[2]));
         SDOT_CUDA(cudaEventElapsedTime(&times[2], ev[2], ev[3]));
-        if ((last_err & DE_SIDE) && side_retries < 4) {
+        if ((last_err & DE_SIDE) && !(last_err & (DE_CAPACITY | DE_DEGEN)) && side_retries < 4) {
             // long rows outgrew the side buffer: grow it and evaluate again
+            // (not when the evaluation failed anyway)
             ++side_retries;
             grow_side(rows);
             if (dim != 3 && mode == DM_MULTI) grow_side(rows_tmp);
@@ -551,11 +552,11 @@ struct sdot_ctx {
     // ---- Newton on the weights (OptimalTransportSolver::solve, .tcc:27-119)
     long long ncap = 0;
     double *t_orig = nullptr, *t_sorted = nullptr, *w_old = nullptr, *dir = nullptr, *rhs = nullptr;
-    double *pcg_buf = nullptr, *red = nullptr;
+    double *pcg_buf = nullptr, *red = nullptr, *mg_buf = nullptr;
     PcgWork pcg;
 
     void free_newton() {
-        dfree(t_orig); dfree(t_sorted); dfree(w_old); dfree(dir); dfree(rhs); dfree(pcg_buf); dfree(red);
+        dfree(t_orig); dfree(t_sorted); dfree(w_old); dfree(dir); dfree(rhs); dfree(pcg_buf); dfree(red); dfree(mg_buf);
         ncap = 0;
     }
     void reserve_newton() {
@@ -564,8 +565,11 @@ struct sdot_ctx {
         ncap = std::max<long long>(n, 1);
         dalloc(t_orig, ncap); dalloc(t_sorted, ncap); dalloc(w_old, ncap); dalloc(dir, ncap); dalloc(rhs, ncap);
         dalloc(pcg_buf, pcg_work_doubles(ncap));
+        dalloc(mg_buf, mg_work_doubles(ncap));
         dalloc(red, 3 * PCG_BLOCKS + 8);
         pcg_bind(pcg, pcg_buf, ncap);
+        pcg.mg = mg_buf;
+        pcg.mg_doubles = mg_work_doubles(ncap);
     }
     // e[0] = max_i |m_i - t_i| / t_i, e[1] = min_i m_i, e[2] = sum_i (m_i - t_i)^2 (sorted order)
     void mass_stats(const double *m, double e[3]) {
@@ -611,6 +615,7 @@ struct sdot_ctx {
             return SDOT_VOID_CELL;
         }
         const double eps0 = 0.5 * std::min(et[1], e[1]);
+        double tau_last = 1.0;
         int status = SDOT_NOT_CONVERGED;
         for (int it = 0;; ++it) {
             rep.max_rel_mass_error = e[0];
@@ -636,12 +641,16 @@ struct sdot_ctx {
             SDOT_CUDA(cudaMemcpyAsync(w_old, d_w, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
             axpby(s_mass, t_sorted, rhs, 1.0, -1.0, n, stream);  // v_values -= masses (.tcc:89-90)
             const PcgResult pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream, 32,
-                                           stream != nullptr);
+                                           stream != nullptr, o.preconditioner == 0);
             rep.pcg_iterations += pr.iterations;
+            rep.pcg_levels = pr.levels;
             if (o.verbosity > 0)
                 fprintf(stderr, "sdot newton %d: pcg %d iterations, relative residual %.3e\n", it, pr.iterations,
                         pr.rel_residual);
-            double tau = 1.0, en[3];
+            // the search starts from 4x the last accepted step length (not
+            // from 1): far from the solution, full steps give huge cells
+            // whose evaluation is slow or overflows; near it tau returns to 1
+            double tau = std::min(1.0, 4.0 * tau_last), en[3];
             bool accepted = false;
             for (int k = 0; k <= 40; ++k) {
                 apply_step(w_old, dir, perm(), tau, d_w, n, stream);  // weights -= dw (.tcc:106-109)
@@ -659,6 +668,7 @@ struct sdot_ctx {
                 if (!o.damping || en[0] <= o.rel_mass_tol ||
                     (en[1] >= eps0 && std::sqrt(en[2]) <= (1.0 - 0.5 * tau) * std::sqrt(e[2]))) {
                     accepted = true;
+                    tau_last = tau;
                     break;
                 }
                 tau *= 0.5;
@@ -1124,7 +1134,7 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
 int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_newton_opts *opts,
                sdot_newton_report *report) {
     return guarded(ctx, [&] {
-        sdot_newton_opts o{150, 1e-10, 20000, 1e-12, 1, 0};
+        sdot_newton_opts o{150, 1e-10, 20000, 1e-12, 1, 0, 0};
         if (opts) o = *opts;
         sdot_newton_report r{};
         ctx->last_error.clear();

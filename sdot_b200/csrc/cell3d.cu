@@ -649,11 +649,13 @@ void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *nex
     SDOT_CUDA(cudaGetLastError());
 }
 
-constexpr long long G3_WARPS = 148;  // warps of the third pass (global memory)
+// warps of the third and fourth passes (faces in global memory, 230 KB and
+// 918 KB per warp: 272 MB of scratch each, shared by the two passes)
+constexpr long long G3_WARPS = 148 * 8;
 
 }  // namespace
 
-constexpr long long G4_WARPS = 32;  // warps of the largest pass
+constexpr long long G4_WARPS = 148 * 2;
 size_t cells3d_scratch_bytes() {
     const size_t a = warp_smem_bytes<4, 64>() * G3_WARPS, b = warp_smem_bytes<8, 128>() * G4_WARPS;
     return (a > b ? a : b) + 256;

@@ -1,5 +1,6 @@
-// Device linear algebra for Newton on the weights: Jacobi-preconditioned
-// conjugate gradient on the Hessian rows (ELL + side buffer, sorted order).
+// Device linear algebra for Newton on the weights: preconditioned conjugate
+// gradient on the Hessian rows (ELL + side buffer, sorted order), with a
+// Jacobi or a multilevel (aggregation V-cycle) preconditioner.
 //
 // Replaces the reference's sparse direct solve EigenSolver::solve
 // (src/sdot/Solvers/EigenSolver.cpp:9-41, Eigen::SimplicialCholesky) used by
@@ -15,7 +16,20 @@ struct PcgWork {
     double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
     double *partial = nullptr;  // PCG_BLOCKS partial sums (x 2)
     double *scal = nullptr;     // device scalars (see solve.cu)
+    double *mg = nullptr;       // multilevel storage (mg_work_doubles(n) doubles), or null
+    size_t mg_doubles = 0;
 };
+
+// One coarse level of the multilevel preconditioner (device arrays).
+struct MgLevel {
+    long long n = 0;
+    int *cnt = nullptr, *col = nullptr;  // ELL rows (width MG_CAP in solve.cu)
+    double *val = nullptr, *dinv = nullptr;
+    double *r = nullptr, *z = nullptr, *zo = nullptr;  // right-hand side, smoothed, output
+};
+
+// Doubles of multilevel storage a solve over n rows needs.
+size_t mg_work_doubles(long long n);
 constexpr int PCG_BLOCKS = 148 * 4;
 
 size_t pcg_work_doubles(long long n);
@@ -25,6 +39,7 @@ struct PcgResult {
     int iterations = 0;
     double rel_residual = 0;
     bool converged = false;
+    int levels = 0;  // multilevel preconditioner levels (0: Jacobi)
 };
 
 // Solves (H + g e_g e_g^T) x = b where H is given by `rows` (sorted order,
@@ -35,8 +50,12 @@ struct PcgResult {
 // iterations, the only host synchronisations).
 // graph: replay full chunks of `check` iterations from one captured CUDA
 // graph (st must be a created stream).
+// multilevel: precondition with one V-cycle over Morton aggregates (needs
+// w.mg); Jacobi when n is small, when w.mg is too small, or when a coarse row
+// outgrows its ELL width.
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                    int max_iter, const PcgWork &w, cudaStream_t st, int check = 32, bool graph = false);
+                    int max_iter, const PcgWork &w, cudaStream_t st, int check = 32, bool graph = false,
+                    bool multilevel = false);
 
 // The same solve on a CSR matrix (device arrays: off[n + 1], col[nnz], val[nnz]).
 struct CsrMat {

@@ -130,3 +130,57 @@ def test_csr_solve_matches_direct_solve(gpu_lib, ref_oracle):
     x_ref = spla.spsolve(sp.csr_matrix((v2, col, off), shape=(n, n)).tocsc(), b)
     assert res <= 1e-13
     assert np.abs(x - x_ref).max() <= 1e-8 * np.abs(x_ref).max()
+
+
+def test_multilevel_and_jacobi_give_the_same_weights(gpu_lib):
+    # the preconditioner changes the CG path, not the Newton solution
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config1()
+    n = len(c["weights"])
+    out = {}
+    for pc in ("multilevel", "jacobi"):
+        g = PowerDiagram(c["positions"], np.zeros(n))
+        g.add_box_shape([0, 0], [1, 1])
+        rep = g.solve_weights(c["target"], rel_mass_tol=1e-11, preconditioner=pc)
+        out[pc] = (g.get_weights(), rep)
+    (wm, rm), (wj, rj) = out["multilevel"], out["jacobi"]
+    assert rm["pcg_levels"] >= 2 and rj["pcg_levels"] == 0
+    assert rm["pcg_iterations"] * 3 < rj["pcg_iterations"]
+    assert np.abs(wm - wj).max() <= 1e-9 * np.abs(wj).max()
+
+
+def test_multilevel_newton_clamped_clusters(gpu_lib):
+    # Diracs clamped onto the box edges (the 1M clustered workload's
+    # definition, here at 300k): sliver cells of mass ~1e-11 at w = 0, where
+    # Jacobi-preconditioned CG stagnates.  Clamping also makes pairs of Diracs
+    # on an edge 4e-8 apart, whose shared face FP64 cannot place finely
+    # enough for 1e-8: the compiled reference with a direct solve stalls at a
+    # relative mass error of 1.5e-6 on this input, so the bound is 1e-5.
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config2(n=300_000)
+    n = len(c["weights"])
+    g = PowerDiagram(c["positions"], np.zeros(n))
+    g.add_box_shape([0, 0], [1, 1])
+    rep = g.solve_weights(c["target"], rel_mass_tol=1e-5)
+    m = g.integrals()
+    assert np.max(np.abs(m - c["target"]) / c["target"]) <= 1e-5
+    assert rep["pcg_levels"] >= 4
+
+
+def test_multilevel_newton_mirrored_clusters(gpu_lib):
+    # the same mix with the clustered Diracs mirrored at the box faces (no
+    # near-coincident pairs): 1e-8 from w = 0
+    from sdot_b200.power_diagram import PowerDiagram
+
+    rng = np.random.default_rng(52)
+    n = 300_000
+    p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng, boundary="reflect")])
+    g = PowerDiagram(p, np.zeros(n))
+    g.add_box_shape([0, 0], [1, 1])
+    t = np.full(n, 1.0 / n)
+    rep = g.solve_weights(t, rel_mass_tol=1e-8)
+    m = g.integrals()
+    assert np.max(np.abs(m - t) / t) <= 1e-8
+    assert rep["pcg_levels"] >= 4
