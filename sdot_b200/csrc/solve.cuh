@@ -16,20 +16,22 @@ struct PcgWork {
     double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
     double *partial = nullptr;  // PCG_BLOCKS partial sums (x 2)
     double *scal = nullptr;     // device scalars (see solve.cu)
-    double *mg = nullptr;       // multilevel storage (mg_work_doubles(n) doubles), or null
+    double *mg = nullptr;       // multilevel storage (mg_work_doubles(n, mg_cap) doubles), or null
     size_t mg_doubles = 0;
+    int mg_cap = 64;            // coarse row width: 64 or 128 (3D)
 };
 
 // One coarse level of the multilevel preconditioner (device arrays).
 struct MgLevel {
     long long n = 0;
-    int *cnt = nullptr, *col = nullptr;  // ELL rows (width MG_CAP in solve.cu)
+    int *cnt = nullptr, *col = nullptr;  // ELL rows (width PcgWork::mg_cap)
     double *val = nullptr, *dinv = nullptr;
     double *r = nullptr, *z = nullptr, *zo = nullptr;  // right-hand side, smoothed, output
 };
 
-// Doubles of multilevel storage a solve over n rows needs.
-size_t mg_work_doubles(long long n);
+// Doubles of multilevel storage a solve over n rows needs (coarse rows of
+// width cap, 64 or 128).
+size_t mg_work_doubles(long long n, int cap);
 constexpr int PCG_BLOCKS = 148 * 4;
 
 size_t pcg_work_doubles(long long n);

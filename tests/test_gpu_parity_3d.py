@@ -127,3 +127,4 @@ def test_config4_density_newton(gpu_lib):
     m = g.integrals()
     assert np.max(np.abs(m - c["target"]) / c["target"]) <= 1e-8
     assert rep["iterations"] <= 20
+    assert rep["pcg_levels"] >= 4  # the multilevel preconditioner ran (coarse rows of 128)
