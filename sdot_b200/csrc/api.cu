@@ -132,6 +132,9 @@ struct sdot_ctx {
     long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
     int *ovf_list = nullptr, *ovf_cnt = nullptr;
     int *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;  // 3D: third pass
+    int *ovf_list3 = nullptr, *ovf_cnt3 = nullptr;  // 3D: fourth pass
+    unsigned char *hint3 = nullptr;                  // 3D: pass of each cell last time
+    bool hint_valid = false;
     void *scratch3 = nullptr;                        // 3D: third pass faces
     unsigned *err = nullptr;
     int *guard = nullptr;
@@ -168,7 +171,7 @@ struct sdot_ctx {
         free_rows(rows);
         free_rows(nb);
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
-        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(err); dfree(guard);
+        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(ovf_list3); dfree(ovf_cnt3); dfree(hint3); dfree(err); dfree(guard);
         if (scratch3) cudaFree(scratch3);
         scratch3 = nullptr;
         if (scratch) cudaFree(scratch);
@@ -213,6 +216,10 @@ struct sdot_ctx {
         if (dim == 3) {
             dalloc(ovf_list2, ecap);
             dalloc(ovf_cnt2, 1);
+            dalloc(ovf_list3, ecap);
+            dalloc(ovf_cnt3, 1);
+            dalloc(hint3, ecap);
+            hint_valid = false;
             SDOT_CUDA(cudaMalloc(&scratch3, cells3d_scratch_bytes()));
         }
         dalloc(err, 1);
@@ -386,6 +393,10 @@ struct sdot_ctx {
         a.ovf_cnt = ovf_cnt;
         a.ovf_list2 = ovf_list2;
         a.ovf_cnt2 = ovf_cnt2;
+        a.ovf_list3 = ovf_list3;
+        a.ovf_cnt3 = ovf_cnt3;
+        a.hint = hint3;
+        a.use_hint = hint_valid ? 1 : 0;
         a.err = err;
         a.guard = guard;
         return a;
@@ -397,6 +408,7 @@ struct sdot_ctx {
             if (dim == 3) {
                 tree3.max_per_leaf = int(max_per_leaf);
                 tree3.build(d_pos, d_w, n, stream);
+                hint_valid = false;  // a new tree order: the hints no longer apply
             } else {
                 tree2.max_per_leaf = int(max_per_leaf);
                 tree2.build(d_pos, d_w, n, stream);
@@ -427,6 +439,7 @@ struct sdot_ctx {
             a.ctd = s_ctd;
             a.rows = rows;
             cells3d_launch(a, scratch3, stream);
+            hint_valid = true;  // every cell of this tree order now has a pass hint
             // get_centroids' mass is the integral itself in 3D
             SDOT_CUDA(cudaMemcpyAsync(s_mass_c, s_mass, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         } else if (mode == DM_MULTI) {

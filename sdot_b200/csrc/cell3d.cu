@@ -559,6 +559,25 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
         }
     }
     bool ok = true;  // the rows fit the side buffer
+    if (status == 0 && A.hint) {
+        // the smallest pass that holds this polyhedron (faces, vertices per face)
+        int faces = 0, maxv = 0;
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) {
+            faces += __popc(__ballot_sync(FULL, C.nv[r] > 0));
+            maxv = max(maxv, C.nv[r]);
+        }
+        for (int o = 16; o > 0; o >>= 1) maxv = max(maxv, __shfl_xor_sync(FULL, maxv, o));
+        const int level = (faces <= 32 && maxv <= 16) ? 0 : (faces <= 64 && maxv <= 32) ? 1
+                          : (faces <= 128 && maxv <= 64) ? 2 : 3;
+        // polyhedra grow larger during the build than at its end, so the
+        // hint is the pass that held this build, lowered by one level at most
+        // when the final polyhedron is smaller (a cell that then overflows
+        // simply moves on to the next pass again)
+        constexpr int pass = FPL == 1 ? 0 : FPL == 2 ? 1 : FPL == 4 ? 2 : 3;
+        const int hint = level >= pass ? pass : pass - 1;
+        if (lane == 0) A.hint[s] = (unsigned char)hint;
+    }
     if (status == 0) {
         const double mass = A.coeff * vol;
         if (lane == 0) {
@@ -611,6 +630,17 @@ __global__ void __launch_bounds__(64) k_cells3d(const Cell3DArgs A, const int *l
     const long long cnt = list ? *list_cnt : A.n;
     for (long long i = gw; i < cnt; i += nwarps) {
         const long long s = list ? list[i] : i;
+        if (!list && A.use_hint && A.hint) {
+            // a cell that needed a larger pass last time goes straight there
+            const int h = A.hint[s];
+            int *to = h == 1 ? next_list : h == 2 ? A.ovf_list2 : h == 3 ? A.ovf_list3 : nullptr;
+            int *tc = h == 1 ? next_cnt : h == 2 ? A.ovf_cnt2 : h == 3 ? A.ovf_cnt3 : nullptr;
+            if (to && tc) {
+                if (lane == 0) to[atomicAdd(tc, 1)] = int(s);
+                __syncwarp();
+                continue;
+            }
+        }
         const int r = cell3d<FPL, MAXV>(A, s, C);
         if (r == 1) {
             if (next_list) {
@@ -650,12 +680,13 @@ void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *nex
 }
 
 // warps of the third and fourth passes (faces in global memory, 230 KB and
-// 918 KB per warp: 272 MB of scratch each, shared by the two passes)
+// 918 KB per warp; the two passes share the scratch, 1.09 GB): 8 per SM,
+// the most that the fourth pass's registers let an SM hold
 constexpr long long G3_WARPS = 148 * 8;
 
 }  // namespace
 
-constexpr long long G4_WARPS = 148 * 2;
+constexpr long long G4_WARPS = 148 * 8;
 size_t cells3d_scratch_bytes() {
     const size_t a = warp_smem_bytes<4, 64>() * G3_WARPS, b = warp_smem_bytes<8, 128>() * G4_WARPS;
     return (a > b ? a : b) + 256;
@@ -665,18 +696,17 @@ void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st) {
     if (a.n == 0) return;
     SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
     SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt2, 0, sizeof(int), st));
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt3, 0, sizeof(int), st));
     if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
     if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
     launch3<1, 16, 2>(a, nullptr, nullptr, a.ovf_list, a.ovf_cnt, a.n, nullptr, 148LL * 7, st);
     // the larger passes take the overflow lists (their lengths are on the
     // device: every warp of the launch reads them)
     launch3<2, 32, 1>(a, a.ovf_list, a.ovf_cnt, a.ovf_list2, a.ovf_cnt2, 148LL * 3, nullptr, 148LL * 3, st);
-    // pass 3 hands its overflow to pass 4 through the first list (pass 2
-    // has consumed it); passes 3 and 4 share the scratch, one after the other
-    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
-    launch3<4, 64, 1>(a, a.ovf_list2, a.ovf_cnt2, a.ovf_list, a.ovf_cnt, G3_WARPS, static_cast<char *>(scratch), G3_WARPS,
-                      st);
-    launch3<8, 128, 1>(a, a.ovf_list, a.ovf_cnt, nullptr, nullptr, G4_WARPS, static_cast<char *>(scratch), G4_WARPS,
+    // passes 3 and 4 share the scratch, one after the other
+    launch3<4, 64, 1>(a, a.ovf_list2, a.ovf_cnt2, a.ovf_list3, a.ovf_cnt3, G3_WARPS, static_cast<char *>(scratch),
+                      G3_WARPS, st);
+    launch3<8, 128, 1>(a, a.ovf_list3, a.ovf_cnt3, nullptr, nullptr, G4_WARPS, static_cast<char *>(scratch), G4_WARPS,
                        st);
 }
 

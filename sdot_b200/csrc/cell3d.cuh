@@ -32,6 +32,13 @@ struct Cell3DArgs {
     int *ovf_cnt = nullptr;
     int *ovf_list2 = nullptr;  // cells handed to the third pass
     int *ovf_cnt2 = nullptr;
+    int *ovf_list3 = nullptr;  // cells handed to the fourth pass
+    int *ovf_cnt3 = nullptr;
+    // per cell (sorted order): the pass (0..3) its last build needed; with
+    // use_hint the first pass sends each cell straight to that pass (the
+    // positions, hence the tree order, must not have changed)
+    unsigned char *hint = nullptr;
+    int use_hint = 0;
     unsigned *err = nullptr;
     int *guard = nullptr;
 };
