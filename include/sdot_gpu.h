@@ -58,6 +58,11 @@ typedef struct sdot_options {
 sdot_ctx *sdot_create(int dim, int precision, const sdot_options *opt);
 void sdot_destroy(sdot_ctx *ctx);
 const char *sdot_last_error(const sdot_ctx *ctx);
+/* Moves the context's device work to `stream` (a cudaStream_t created on the
+ * context's device; NULL: a stream of the context's own).  Work already queued
+ * on the previous stream is waited for first.  No reference counterpart: the
+ * serving loop uses it to run its largest requests on a high-priority stream. */
+int sdot_set_stream(sdot_ctx *ctx, void *stream);
 
 /* ---- Diracs --------------------------------------------------------------
  * Replaces SpZGrid::update( positions, weights, nb_diracs, ... )

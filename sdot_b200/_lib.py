@@ -85,6 +85,7 @@ SIGNATURES = {
     "sdot_set_image_density": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
     "sdot_set_polynomial_density": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "sdot_clear_domain": (ctypes.c_int, [_P]),
+    "sdot_set_stream": (ctypes.c_int, [_P, _P]),
     "sdot_normalize_domain": (ctypes.c_int, [_P]),
     "sdot_domain_measure": (ctypes.c_int, [_P, _P]),
     "sdot_set_ball_cut": (ctypes.c_int, [_P, ctypes.c_int]),

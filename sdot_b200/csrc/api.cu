@@ -792,6 +792,23 @@ void sdot_destroy(sdot_ctx *ctx) { delete ctx; }
 
 const char *sdot_last_error(const sdot_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
+int sdot_set_stream(sdot_ctx *ctx, void *stream) {
+    return guarded(ctx, [&] {
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (stream) {
+            if (ctx->own_stream) SDOT_CUDA(cudaStreamDestroy(ctx->stream));
+            ctx->own_stream = false;
+            ctx->stream = static_cast<cudaStream_t>(stream);
+        } else if (!ctx->own_stream) {
+            cudaStream_t s = nullptr;
+            SDOT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            ctx->stream = s;
+            ctx->own_stream = true;
+        }
+        return int(SDOT_OK);
+    });
+}
+
 int sdot_set_diracs(sdot_ctx *ctx, const double *positions, const double *weights, int64_t n, int mem_space) {
     return guarded(ctx, [&] {
         if (n < 0 || (n > 0 && (!positions || !weights))) throw BadArg("bad Dirac arrays");
