@@ -770,7 +770,8 @@ constexpr int smem_extra_halves() {
 }
 
 template <int MODE, bool BALL>
-__global__ void __launch_bounds__(T2D_MAX) k_cells2d(const Cell2DArgs A) {
+// six blocks of T2D_MAX threads per SM: at most 85 registers per thread
+__global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d(const Cell2DArgs A) {
     extern __shared__ double smem[];
     constexpr int CAP = CAP_FAST_2D;
     const int t = threadIdx.x, T2D = blockDim.x;
