@@ -212,6 +212,9 @@ int sdot_csr_solve(const int64_t *offsets, const int64_t *columns, const double 
  *   - the first call on each device looks up that device's scratch array
  *     (cudaGetSymbolAddress, with the device current), so make the first call
  *     on a device before any stream capture on that device;
+ *   - that address is kept for the life of the process: resetting the device
+ *     (cudaDeviceReset) between calls is not supported, since the array may
+ *     then move and the kept address would be stale;
  *   - calls whose work overlaps on one device (several threads or streams)
  *     race on the shared scratch: the caller serialises them.
  * Other arguments and results as sdot_csr_solve.                            */

@@ -15,7 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libsdot_ref.so")
-REF_TREE = "/root/reference"
+# The reference checkout: $SDOT_REFERENCE_DIR, else a checkout named
+# "reference" beside this repository's root directory.
+REF_TREE = os.environ.get("SDOT_REFERENCE_DIR") or os.path.join(os.path.dirname(HERE), os.pardir, "reference")
 
 _lib = None
 

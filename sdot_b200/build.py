@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libsdot_b200.so")
 SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "cell3d.cu", "csr.cu", "solve.cu", "api.cu", "server.cu", "peaks.cu",
            "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
 
 
@@ -35,18 +35,40 @@ def needs_rebuild():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def _compile(src, obj, extra):
+    cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return cmd, r
+
+
 def build(force=False, verbose=False, extra=()):
+    """Compiles every source to an object file (in parallel, one nvcc per
+    file), then links the shared library."""
     if not force and not needs_rebuild():
         return LIB
-    cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-o", LIB + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    jobs = [(os.path.join(CSRC, s), os.path.join(objdir, s.replace(".cu", ".o"))) for s in SOURCES]
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda j: _compile(j[0], j[1], extra), jobs))
+    failed = False
+    for cmd, r in results:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        if r.returncode != 0:
+            failed = True
+            sys.stderr.write(r.stdout + r.stderr)
+        elif verbose and (r.stdout or r.stderr):
+            sys.stderr.write(r.stdout + r.stderr)
+    if failed:
+        raise RuntimeError("nvcc failed building libsdot_b200.so")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *[o for _, o in jobs]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libsdot_b200.so")
-    if verbose and (r.stdout or r.stderr):
-        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed linking libsdot_b200.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

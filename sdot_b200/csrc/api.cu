@@ -130,15 +130,31 @@ struct sdot_ctx {
     double *o_mass = nullptr, *o_mass_c = nullptr, *o_ctd = nullptr;
     Rows rows, nb;             // Hessian rows, boundary id lists (sorted order)
     long long *cnt_orig = nullptr, *offsets = nullptr, *nb_offsets = nullptr;
+    // Status words of one evaluation, kept together in device memory so that
+    // one copy brings them all back (into the pinned mirror hstat).
+    struct DevStatus {
+        long long nnz;               // Hessian entries (the last CSR offset)
+        unsigned long long n_void;   // empty cells
+        unsigned err;                // DevErr bits
+        int ovf;                     // cells handed to the overflow tier
+        int guard[3];                // first failed guard (code, cell, value)
+        int pad;
+    };
+    DevStatus *dstat = nullptr, *hstat = nullptr;
     int *ovf_list = nullptr, *ovf_cnt = nullptr;
     int *ovf_list2 = nullptr, *ovf_cnt2 = nullptr;  // 3D: third pass
     int *ovf_list3 = nullptr, *ovf_cnt3 = nullptr;  // 3D: fourth pass
     unsigned char *hint3 = nullptr;                  // 3D: pass of each cell last time
     bool hint_valid = false;
     void *scratch3 = nullptr;                        // 3D: third pass faces
-    unsigned *err = nullptr;
-    int *guard = nullptr;
+    unsigned *err = nullptr;   // &dstat->err
+    int *guard = nullptr;      // dstat->guard
     long long item_nv = 0;
+    // device staging of the CSR columns / values and neighbour ids that go to
+    // host buffers (int64 + double per entry), grown with nnz
+    long long *stage_i = nullptr;
+    double *stage_v = nullptr;
+    long long stage_cap = 0;
     std::vector<int> item_off_h;  // vertex offsets of the shapes (several shapes)
     void *scratch = nullptr, *scan_tmp = nullptr;
     // several shapes: one cell pass per shape into these, summed into the above
@@ -163,6 +179,7 @@ struct sdot_ctx {
         free_newton();
         free_multi();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
+        if (hstat) cudaFreeHost(hstat);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
@@ -171,7 +188,13 @@ struct sdot_ctx {
         free_rows(rows);
         free_rows(nb);
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
-        dfree(ovf_list); dfree(ovf_cnt); dfree(ovf_list2); dfree(ovf_cnt2); dfree(ovf_list3); dfree(ovf_cnt3); dfree(hint3); dfree(err); dfree(guard);
+        dfree(ovf_list); dfree(ovf_list2); dfree(ovf_cnt2); dfree(ovf_list3); dfree(ovf_cnt3); dfree(hint3);
+        dfree(dstat);
+        ovf_cnt = nullptr;
+        err = nullptr;
+        guard = nullptr;
+        dfree(stage_i); dfree(stage_v);
+        stage_cap = 0;
         if (scratch3) cudaFree(scratch3);
         scratch3 = nullptr;
         if (scratch) cudaFree(scratch);
@@ -212,7 +235,11 @@ struct sdot_ctx {
         dalloc(cnt_orig, ecap + 1);
         dalloc(offsets, ecap + 1);
         dalloc(ovf_list, ecap);
-        dalloc(ovf_cnt, 1);
+        dalloc(dstat, 1);
+        ovf_cnt = &dstat->ovf;
+        err = &dstat->err;
+        guard = dstat->guard;
+        if (!hstat) SDOT_CUDA(cudaMallocHost(reinterpret_cast<void **>(&hstat), sizeof(DevStatus)));
         if (dim == 3) {
             dalloc(ovf_list2, ecap);
             dalloc(ovf_cnt2, 1);
@@ -222,8 +249,6 @@ struct sdot_ctx {
             hint_valid = false;
             SDOT_CUDA(cudaMalloc(&scratch3, cells3d_scratch_bytes()));
         }
-        dalloc(err, 1);
-        dalloc(guard, 3);
         SDOT_CUDA(cudaMalloc(&scratch, cells2d_scratch_bytes()));
         SDOT_CUDA(cudaMalloc(&scan_tmp, scan_tmp_size(ecap + 1, sizeof(long long))));
     }
@@ -428,8 +453,7 @@ struct sdot_ctx {
         check_domain();
         reserve_eval();
         if (!ev[0]) for (auto &e : ev) SDOT_CUDA(cudaEventCreate(&e));
-        SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
-        SDOT_CUDA(cudaMemsetAsync(guard, 0, 3 * sizeof(int), stream));
+        SDOT_CUDA(cudaMemsetAsync(dstat, 0, sizeof(DevStatus), stream));
         SDOT_CUDA(cudaEventRecord(ev[0], stream));
         ensure_tree();
         SDOT_CUDA(cudaEventRecord(ev[1], stream));
@@ -459,11 +483,17 @@ struct sdot_ctx {
         unpermute(s_mass_c, o_mass_c, n, 1, perm(), stream);
         unpermute(s_ctd, o_ctd, n, dim, perm(), stream);
         SDOT_CUDA(cudaEventRecord(ev[3], stream));
-        SDOT_CUDA(cudaMemcpyAsync(&nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
-        SDOT_CUDA(cudaMemcpyAsync(&last_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-        SDOT_CUDA(cudaMemcpyAsync(&last_ovf, ovf_cnt, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        SDOT_CUDA(cudaMemcpyAsync(last_guard, guard, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        // the status block (nnz, empty cells, error bits, overflow count,
+        // guard) comes back in one copy
+        SDOT_CUDA(cudaMemcpyAsync(&dstat->nnz, offsets + n, sizeof(long long), cudaMemcpyDeviceToDevice, stream));
+        count_zeros(s_mass, n, &dstat->n_void, stream);
+        SDOT_CUDA(cudaMemcpyAsync(hstat, dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaStreamSynchronize(stream));
+        nnz = hstat->nnz;
+        n_void = (long long)hstat->n_void;
+        last_err = hstat->err;
+        last_ovf = hstat->ovf;
+        for (int k = 0; k < 3; ++k) last_guard[k] = hstat->guard[k];
         SDOT_CUDA(cudaEventElapsedTime(&times[0], ev[0], ev[1]));
         SDOT_CUDA(cudaEventElapsedTime(&times[1], ev[1], ev[2]));
         SDOT_CUDA(cudaEventElapsedTime(&times[2], ev[2], ev[3]));
@@ -561,6 +591,15 @@ struct sdot_ctx {
     }
 
     void mark_dirty() { eval_dirty = nb_dirty = true; }
+
+    // staging buffers of at least `count` entries (25% headroom when grown)
+    void reserve_stage(long long count) {
+        if (count <= stage_cap && stage_i) return;
+        const long long cap2 = count + count / 4 + 1024;
+        dalloc(stage_i, size_t(cap2));
+        dalloc(stage_v, size_t(cap2));
+        stage_cap = cap2;
+    }
 
     // ---- Newton on the weights (OptimalTransportSolver::solve, .tcc:27-119)
     long long ncap = 0;
@@ -1100,35 +1139,27 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
         const long long n = ctx->n, nnz = ctx->nnz;
         long long *dcols = reinterpret_cast<long long *>(columns);
         double *dvals = values;
-        long long *tmp_c = nullptr;
-        double *tmp_v = nullptr;
         if (mem_space != SDOT_DEVICE) {
-            dalloc(tmp_c, nnz);
-            dalloc(tmp_v, nnz);
-            dcols = tmp_c;
-            dvals = tmp_v;
+            // host outputs: written on the device into the context's staging
+            // buffers, then copied
+            ctx->reserve_stage(nnz);
+            dcols = ctx->stage_i;
+            dvals = ctx->stage_v;
         }
         csr_write(ctx->rows, n, ctx->perm(), ctx->offsets, dcols, dvals, ctx->stream);
-        if (mem_space != SDOT_DEVICE) {
-            SDOT_CUDA(cudaMemcpyAsync(columns, tmp_c, nnz * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
-            SDOT_CUDA(cudaMemcpyAsync(values, tmp_v, nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        }
         ctx->copy_out(offsets, ctx->offsets, size_t(n + 1) * sizeof(long long), mem_space);
         ctx->copy_out(masses, ctx->o_mass, size_t(n) * sizeof(double), mem_space);
+        if (mem_space != SDOT_DEVICE) {
+            SDOT_CUDA(cudaMemcpyAsync(columns, dcols, nnz * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(values, dvals, nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        }
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
-        dfree(tmp_c);
-        dfree(tmp_v);
         *nnz_inout = nnz;
-        if (stop_if_void) {
-            // reference: any v == 0 -> 1 (get_der_integrals_wrt_weights.h:93-96)
-            std::vector<double> m(n);
-            SDOT_CUDA(cudaMemcpyAsync(m.data(), ctx->o_mass, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
-            for (double v : m)
-                if (v == 0) {
-                    ctx->last_error = "void cell";
-                    return int(SDOT_VOID_CELL);
-                }
+        if (stop_if_void && ctx->n_void > 0) {
+            // reference: any v == 0 -> 1 (get_der_integrals_wrt_weights.h:93-96);
+            // the empty cells were counted on the device by the evaluation
+            ctx->last_error = "void cell";
+            return int(SDOT_VOID_CELL);
         }
         return int(SDOT_OK);
     });
@@ -1146,17 +1177,15 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
         if (!offsets) throw BadArg("null offsets");
         const long long n = ctx->n, tot = ctx->nb_total;
         long long *dids = reinterpret_cast<long long *>(ids);
-        long long *tmp = nullptr;
         if (mem_space != SDOT_DEVICE) {
-            dalloc(tmp, tot);
-            dids = tmp;
+            ctx->reserve_stage(tot);
+            dids = ctx->stage_i;
         }
         nb_write(ctx->nb, n, ctx->perm(), ctx->nb_offsets, dids, ctx->stream);
         if (mem_space != SDOT_DEVICE)
-            SDOT_CUDA(cudaMemcpyAsync(ids, tmp, tot * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(ids, dids, tot * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
         ctx->copy_out(offsets, ctx->nb_offsets, size_t(n + 1) * sizeof(long long), mem_space);
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
-        dfree(tmp);
         *count_inout = tot;
         return int(SDOT_OK);
     });

@@ -762,6 +762,17 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
     return true;
 }
 
+// Hands cell s to the warp tier.  The list holds n entries and one launch
+// appends each cell at most once; the bound check turns a count that was not
+// reset between launches into an error instead of a write past the list.
+__device__ void push_overflow(const Cell2DArgs &A, long long s) {
+    const int k = atomicAdd(A.ovf_cnt, 1);
+    if (k < A.n)
+        A.ovf_list[k] = int(s);
+    else
+        flag_error(A.err, DE_CAPACITY);
+}
+
 // shared memory of the fast kernels, in half-doubles per vertex slot and
 // thread beyond the polygon: the per-edge accumulators of the image mode
 template <int MODE>
@@ -790,8 +801,7 @@ __global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d(const Cell2DArgs A) {
         if (A.rows.cnt) A.rows.cnt[s] = row.cnt;
         if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
     } else {
-        const int k = atomicAdd(A.ovf_cnt, 1);
-        A.ovf_list[k] = int(s);
+        push_overflow(A, s);
     }
 }
 
@@ -831,10 +841,7 @@ __global__ void __launch_bounds__(T2D_MAX) k_cells2d_mixed(const Cell2DArgs A) {
             if (A.nb.cnt) A.nb.cnt[s] = nbo.cnt;
         }
     }
-    if (!ok) {
-        const int k = atomicAdd(A.ovf_cnt, 1);
-        A.ovf_list[k] = int(s);
-    }
+    if (!ok) push_overflow(A, s);
 }
 
 // Polygon, accumulators and row buffers of one warp of the warp tier,
@@ -1012,13 +1019,10 @@ __global__ void __launch_bounds__(128) k_cells2d_wtier(const Cell2DArgs A, doubl
     }
 }
 
-// Block size of the fast kernels, picked once per kernel variant on the
+// The block size of the fast kernels is picked once per kernel variant and
 // device by timing the candidates on the first evaluation large enough to
 // tell them apart (the results do not depend on it: one thread builds one
 // cell whatever the block).
-struct BlockTuner {
-    int best = 0;
-};
 
 template <int MODE, bool BALL>
 size_t fast_smem(int bs, bool mixed) {
@@ -1038,47 +1042,53 @@ void launch_fast(const Cell2DArgs &a, int bs, cudaStream_t st) {
     SDOT_CUDA(cudaGetLastError());
 }
 
+// Counters the fast kernel appends to: zeroed before every launch of it.
+void reset_overflow(const Cell2DArgs &a, cudaStream_t st) {
+    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
+    if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
+    if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
+}
+
 template <int MODE, bool BALL>
 void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
-    static bool attr_set = false;
-    if (!attr_set) {
+    static PerDevice<int> attr_set;
+    attr_set.once([] {
         SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(fast_smem<MODE, BALL>(T2D_MAX, false))));
         SDOT_CUDA(cudaFuncSetAttribute(k_cells2d_mixed<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(fast_smem<MODE, BALL>(T2D_MAX, true))));
-        attr_set = true;
-    }
-    static BlockTuner tuner[2];  // FP64, mixed
-    BlockTuner &tu = tuner[a.mixed ? 1 : 0];
-    if (!tu.best) {
-        if (a.n >= (1 << 17)) {
-            // time each candidate on this evaluation's cells; the outputs of
-            // the trial runs are all rewritten by the run that follows
-            const int cand[3] = {32, 64, 128};
-            float best_ms = 0;
-            cudaEvent_t e0, e1;
-            SDOT_CUDA(cudaEventCreate(&e0));
-            SDOT_CUDA(cudaEventCreate(&e1));
-            for (int bs : cand) {
-                SDOT_CUDA(cudaEventRecord(e0, st));
-                launch_fast<MODE, BALL>(a, bs, st);
-                SDOT_CUDA(cudaEventRecord(e1, st));
-                SDOT_CUDA(cudaEventSynchronize(e1));
-                float ms = 0;
-                SDOT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                if (!tu.best || ms < best_ms) {
-                    tu.best = bs;
-                    best_ms = ms;
-                }
+    });
+    static PerDevice<int> tuned[2];  // best block size per device: FP64, mixed
+    PerDevice<int> &tu = tuned[a.mixed ? 1 : 0];
+    int best = tu.get();
+    if (!best && a.n >= (1 << 17)) {
+        // time each candidate on this evaluation's cells; every output of the
+        // trial runs is rewritten by the run that follows, and the overflow
+        // counters are zeroed before each run
+        const int cand[3] = {32, 64, 128};
+        float best_ms = 0;
+        cudaEvent_t e0, e1;
+        SDOT_CUDA(cudaEventCreate(&e0));
+        SDOT_CUDA(cudaEventCreate(&e1));
+        for (int bs : cand) {
+            reset_overflow(a, st);
+            SDOT_CUDA(cudaEventRecord(e0, st));
+            launch_fast<MODE, BALL>(a, bs, st);
+            SDOT_CUDA(cudaEventRecord(e1, st));
+            SDOT_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            SDOT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (!best || ms < best_ms) {
+                best = bs;
+                best_ms = ms;
             }
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
-            if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
-            if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
         }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        tu.set(best);
     }
-    launch_fast<MODE, BALL>(a, tu.best ? tu.best : 64, st);
+    reset_overflow(a, st);
+    launch_fast<MODE, BALL>(a, best ? best : 64, st);
     k_cells2d_wtier<MODE, BALL><<<WTIER_WARPS / 4, 128, 0, st>>>(a, static_cast<double *>(scratch), WTIER_WARPS,
                                                                   a.ovf_list, a.ovf_cnt);
     note_launch();
@@ -1101,9 +1111,6 @@ size_t cells2d_scratch_bytes() {
 
 void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
     if (a.n == 0) return;
-    SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
-    if (a.rows.side_used) SDOT_CUDA(cudaMemsetAsync(a.rows.side_used, 0, sizeof(unsigned long long), st));
-    if (a.nb.side_used) SDOT_CUDA(cudaMemsetAsync(a.nb.side_used, 0, sizeof(unsigned long long), st));
     const bool ball = a.ball != 0;
     if (a.mode == DM_SINGLE) {
         if (ball) launch_all<DM_SINGLE, true>(a, scratch, st); else launch_all<DM_SINGLE, false>(a, scratch, st);

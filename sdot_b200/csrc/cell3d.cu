@@ -665,11 +665,11 @@ template <int FPL, int MAXV, int WPB>
 void launch3(const Cell3DArgs &a, const int *list, const int *list_cnt, int *next_list, int *next_cnt, long long ncells,
              char *gscratch, long long max_blocks, cudaStream_t st) {
     const size_t smem = gscratch ? 0 : warp_smem_bytes<FPL, MAXV>() * WPB;
-    static bool attr = false;
-    if (!attr && !gscratch) {
-        SDOT_CUDA(cudaFuncSetAttribute(k_cells3d<FPL, MAXV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        attr = true;
-    }
+    static PerDevice<int> attr;
+    if (!gscratch)
+        attr.once([&] {
+            SDOT_CUDA(cudaFuncSetAttribute(k_cells3d<FPL, MAXV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        });
     long long blocks = (ncells + WPB - 1) / WPB;
     if (blocks > max_blocks) blocks = max_blocks;
     if (blocks < 1) blocks = 1;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 namespace sdot {
@@ -74,6 +75,43 @@ __host__ __device__ inline void check_fail(int code, int line, long long value) 
 #endif
 
 inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+// Per-device state of a kernel launcher (shared-memory attributes, tuned block
+// sizes): one slot per device ordinal, read and written under one mutex, so
+// that contexts on several devices, or several threads, can launch at once.
+constexpr int kDeviceSlots = 64;
+template <class T>
+struct PerDevice {
+    std::mutex m;
+    T slot[kDeviceSlots] = {};
+    // the current device's slot index (throws on an ordinal beyond the table)
+    static int device() {
+        int d = 0;
+        SDOT_CUDA(cudaGetDevice(&d));
+        if (d < 0 || d >= kDeviceSlots) throw CudaError{cudaErrorInvalidDevice, "device ordinal beyond 64"};
+        return d;
+    }
+    T get() {
+        const int d = device();
+        std::lock_guard<std::mutex> g(m);
+        return slot[d];
+    }
+    void set(const T &v) {
+        const int d = device();
+        std::lock_guard<std::mutex> g(m);
+        slot[d] = v;
+    }
+    // runs f() unless this device's slot is already set, then sets it (f runs
+    // under the lock: concurrent first calls on one device wait for it)
+    template <class F>
+    void once(const F &f) {
+        const int d = device();
+        std::lock_guard<std::mutex> g(m);
+        if (slot[d]) return;
+        f();
+        slot[d] = T(1);
+    }
+};
 
 // Process-wide count of this library's kernel launches (sdot_kernel_launches).
 void note_launch();

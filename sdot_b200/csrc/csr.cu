@@ -107,6 +107,14 @@ __global__ void k_unpermute(const double *in, double *out, long long n, int d, c
     for (int k = 0; k < d; ++k) out[i * d + k] = in[s * d + k];
 }
 
+// number of zero entries (empty cells), added to *count
+__global__ void k_count_zeros(const double *m, long long n, unsigned long long *count) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool z = s < n && m[s] == 0.0;
+    const unsigned b = __ballot_sync(0xffffffffu, z);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, (unsigned long long)__popc(b));
+}
+
 // ---- domains of several shapes: one cell pass per shape, summed here
 __global__ void k_rows_clear(Rows R, long long n) {
     const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -229,6 +237,13 @@ void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass
 void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st) {
     if (n <= 0) return;
     k_ctd_final2<<<ceil_div(n, TB), TB, 0, st>>>(ctd, mom, mass_c, n);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+
+void count_zeros(const double *m, long long n, unsigned long long *count, cudaStream_t st) {
+    if (n <= 0) return;
+    k_count_zeros<<<ceil_div(n, TB), TB, 0, st>>>(m, n, count);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }

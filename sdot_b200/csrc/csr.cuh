@@ -27,6 +27,8 @@ void rows_append(const Rows &dst, const Rows &src, long long n, unsigned *err, c
 void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
                  const double *t_ctd, long long n, cudaStream_t st);
 void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st);
+// *count += number of i < n with m[i] == 0 (the empty cells)
+void count_zeros(const double *m, long long n, unsigned long long *count, cudaStream_t st);
 // out[idx[s] * d + k] = in[s * d + k]
 void unpermute(const double *in, double *out, long long n, int d, const int *idx, cudaStream_t st);
 

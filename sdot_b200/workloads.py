@@ -103,42 +103,3 @@ def serving_requests(count=2000, rate_hz=50.0, seed_salt=0):
         p = clustered_points(n, dim, r, boundary="reflect") if clustered else uniform_points(n, dim, r)
         reqs.append({"arrival_s": float(t[k]), "dim": dim, "n": n, "clustered": bool(clustered), "positions": p})
     return reqs
-
-
-def _evaluate_main(argv):
-    """python -m sdot_b200.workloads CASE REPS: builds one named workload and
-    evaluates it REPS times (masses, centroids, Hessian), printing the stage
-    times of each evaluation; the profiling commands run this.  CASE is
-    c2_N (the 2D clustered mix at N Diracs), c4_N (the 3D mix with its
-    density) or serving_K (request K < 100 of the seeded 100-request serving
-    stream, w = 0)."""
-    from .power_diagram import PowerDiagram
-
-    case, reps = argv[0], int(argv[1])
-    density = None
-    if case.startswith("c2_"):
-        c = config2(n=int(case[3:]))
-        p, w = c["positions"], c["weights"]
-    elif case.startswith("c4_"):
-        c = config4(n=int(case[3:]))
-        p, w, density = c["positions"], c["weights"], c["density"]
-    elif case.startswith("serving_"):
-        r = serving_requests(count=100)[int(case[8:])]
-        p, w = r["positions"], np.zeros(r["n"])
-    else:
-        raise SystemExit(f"unknown case {case}")
-    dim = p.shape[1]
-    g = PowerDiagram(p, w)
-    g.add_box_shape(np.zeros(dim), np.ones(dim))
-    if density is not None:
-        g.set_polynomial_density(density)
-    for k in range(reps):
-        g.set_weights(w)
-        g.evaluate()
-        print(case, k, {key: round(float(v), 3) for key, v in g.last_timings().items()}, flush=True)
-
-
-if __name__ == "__main__":
-    import sys
-
-    _evaluate_main(sys.argv[1:])

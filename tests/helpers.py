@@ -51,3 +51,18 @@ def compare_csr(g, r, rtol, floor):
 
 def neighbor_sets(off, ids):
     return [frozenset(int(x) for x in ids[off[i]:off[i + 1]]) for i in range(len(off) - 1)]
+
+
+def neighbor_set_mismatches(off_a, ids_a, off_b, ids_b):
+    """Rows whose sets of ids differ (vectorised: one unique-sort of
+    (row, id) keys per side).  Returns the sorted array of those rows."""
+    n = len(off_a) - 1
+    assert len(off_b) - 1 == n
+
+    def keys(off, ids):
+        rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+        return np.unique(rows * (np.int64(n) + 8) + (np.asarray(ids, dtype=np.int64) + 4))
+
+    ka, kb = keys(off_a, ids_a), keys(off_b, ids_b)
+    only = np.setxor1d(ka, kb, assume_unique=True)
+    return np.unique(only // (np.int64(n) + 8))

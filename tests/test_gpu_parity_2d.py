@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from sdot_b200 import workloads
-from tests.helpers import assert_close, compare_csr, make_pair, neighbor_sets
+from tests.helpers import assert_close, compare_csr, make_pair, neighbor_set_mismatches
 
 pytestmark = pytest.mark.gpu
 
@@ -43,9 +43,12 @@ def check_all(gpu, ref, n, rtol=RTOL, rtol_hess=None, check_nb=True):
     if check_nb:
         go, gi = gpu.neighbors()
         ro2, ri = ref.neighbors()
-        gs, rs = neighbor_sets(go, gi), neighbor_sets(ro2, ri)
-        bad = [i for i in range(n) if gs[i] != rs[i]]
-        assert not bad, f"{len(bad)} neighbour sets differ, first {bad[:5]}: {gs[bad[0]]} vs {rs[bad[0]]}"
+        bad = neighbor_set_mismatches(go, gi, ro2, ri)
+        if len(bad):
+            k = int(bad[0])
+            raise AssertionError(f"{len(bad)} neighbour sets differ, first {bad[:5].tolist()}: "
+                                 f"{sorted(set(gi[go[k]:go[k + 1]].tolist()))} vs "
+                                 f"{sorted(set(ri[ro2[k]:ro2[k + 1]].tolist()))}")
 
 
 @pytest.mark.parametrize("n", [1, 2, 7, 100, 2000])

@@ -51,10 +51,14 @@ def solve_noalloc(lib, d_off, d_col, d_val, d_b, d_x, n, stream):
     return st, msg.value.decode(), it.value, res.value
 
 
-def test_noalloc_solve_matches_existing_entry_point(gpu_lib):
+def check_two_calls(gpu_lib, n):
+    """Solves one Hessian twice in a row through the allocation-free entry
+    point; both results must match sdot_csr_solve, and the second call must
+    leave the device's free memory unchanged (an allocation made inside the
+    library would not pass through torch's caching allocator, but it would
+    show up in cudaMemGetInfo at the driver's granularity)."""
     import torch
 
-    n = 10_000
     off, col, val, b = hessian_c1(n)
     x_ref = solve_existing(gpu_lib, off, col, val, b)
     dev = torch.device("cuda", 0)
@@ -64,15 +68,29 @@ def test_noalloc_solve_matches_existing_entry_point(gpu_lib):
     d_b = torch.from_numpy(b).to(dev)
     stream = torch.cuda.Stream(device=dev)
     scale = np.abs(x_ref).max()
+    d_xs = [torch.full((n,), float("nan"), dtype=torch.float64, device=dev) for _ in range(2)]
     for call in range(2):  # two calls in a row reuse the same scratch
-        d_x = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
-        st, msg, it, res = solve_noalloc(gpu_lib, d_off, d_col, d_val, d_b, d_x, n, stream.cuda_stream)
+        free0 = torch.cuda.mem_get_info(dev)[0]
+        st, msg, it, res = solve_noalloc(gpu_lib, d_off, d_col, d_val, d_b, d_xs[call], n, stream.cuda_stream)
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info(dev)[0]
         assert st == 0, msg
         assert res <= 1e-13 and it > 0
-        x = d_x.cpu().numpy()
+        if call == 1:
+            assert free1 == free0, f"free device memory changed by {free0 - free1} bytes during the call"
+        x = d_xs[call].cpu().numpy()
         err = np.abs(x - x_ref).max() / scale
         assert err <= RTOL, f"call {call}: max difference {err:.3e} of max |x|"
+
+
+def test_noalloc_solve_matches_existing_entry_point(gpu_lib):
+    check_two_calls(gpu_lib, 10_000)
+
+
+def test_noalloc_solve_at_the_row_limit(gpu_lib):
+    """n = SDOT_NOALLOC_MAX_ROWS: every work vector of the scratch array in use."""
+    check_two_calls(gpu_lib, 65_536)
 
 
 def test_noalloc_rejects_rows_beyond_the_limit(gpu_lib):
