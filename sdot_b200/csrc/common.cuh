@@ -1,6 +1,7 @@
 // Shared definitions for the sdot_b200 CUDA library (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>

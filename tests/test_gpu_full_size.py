@@ -15,7 +15,13 @@ parity tests):
     collinear Diracs on the box edges, whose bisectors are nearly parallel,
     so a vertex carries an error of eps / sin(angle).  Masses and centroids
     are held to 1e-11 and the Hessian to 1e-9 (ten times that spread).
-  * C3: arcs use device atan2 / sin / cos (a few ulp from the host's): 1e-11.
+  * C3: where a cell edge is nearly tangent to the clipping disc, the
+    edge-circle intersection is the root of a discriminant at rounding level,
+    so inputs that differ by one ulp move it by ~sqrt(eps * r) along the edge.
+    The reference and the C restatement differ on this input by 6.8e-10 in
+    the masses (54 cells above 1e-11), 1.5e-13 in the centroids and 6.9e-11 in
+    the Hessian values: masses and Hessian are held to 1e-9, centroids to
+    1e-11.
   * C4: 1e-12 for volumes and centroids, 1e-11 for the Hessian, the bounds of
     the 20k-Dirac 3D test.
 Neighbour sets and CSR patterns must match exactly.
@@ -45,7 +51,7 @@ def test_config3_full_size(gpu_lib, ref_oracle):
     c = workloads.config3()
     n = len(c["weights"])
     gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle, radial_func="in_ball_w05", image=c["image"])
-    check_all(gpu, ref, n, rtol=1e-11)
+    check_all(gpu, ref, n, rtol=1e-9, rtol_hess=1e-9, rtol_ctd=1e-11)
 
 
 def test_config4_geometry_full_size(gpu_lib, ref_oracle):

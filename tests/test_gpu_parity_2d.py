@@ -21,8 +21,9 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-12
 
 
-def check_all(gpu, ref, n, rtol=RTOL, rtol_hess=None, check_nb=True):
+def check_all(gpu, ref, n, rtol=RTOL, rtol_hess=None, check_nb=True, rtol_ctd=None):
     rtol_hess = rtol if rtol_hess is None else rtol_hess
+    rtol_ctd = rtol if rtol_ctd is None else rtol_ctd
     m_r = ref.integrals()
     mean = max(float(np.abs(m_r).mean()), 1e-300)
     m_g = gpu.integrals()
@@ -30,7 +31,7 @@ def check_all(gpu, ref, n, rtol=RTOL, rtol_hess=None, check_nb=True):
     c_g, mc_g = gpu.centroids(with_masses=True)
     c_r, mc_r = ref.centroids(with_masses=True)
     assert_close(mc_g, mc_r, rtol, mean, "centroid masses")
-    assert_close(c_g, c_r, rtol, 1.0, "centroids")
+    assert_close(c_g, c_r, rtol_ctd, 1.0, "centroids")
     off, col, val, mas = gpu.der_integrals_wrt_weights()
     err, ro, rc, rv, rm = ref.der_integrals_wrt_weights()
     assert err == 0
