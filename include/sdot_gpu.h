@@ -128,6 +128,27 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
  * domain edge, -2 for a disc arc.  Two-phase like the Hessian.               */
 int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *count_inout, int mem_space);
 
+/* ---- rasterisation ----------------------------------------------------------
+ * get_image_integrals( res, grid, bounds, positions, weights, n, rf, min_pt,
+ *   max_pt, nbp )  (get_image_integrals.h:16-78): for the raster of
+ * nb_pixels[0] x nb_pixels[1] pixels over the box [min_pt, max_pt], out
+ * (double[3 * pixels], pixel index x-fastest) receives per pixel
+ * (sum_i m_i x_i, sum_i m_i y_i, sum_i m_i), m_i the integral of cell i (with
+ * the domain's density, after the disc clip with InBallW05) over the pixel.
+ * The per-pixel sums run in no fixed order (atomic additions): results agree
+ * with the reference to rounding, not bit for bit.  2D, box / convex-shape
+ * domains (SDOT_UNSUPPORTED with an image density).                          */
+int sdot_get_image_integrals(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const int64_t *nb_pixels,
+                             double *out, int mem_space);
+/* get_image_of_cell_nums( res, grid, bounds, positions, weights, n, rf,
+ *   min_pt, max_pt, nbp )  (get_image_of_cell_nums.h:13-80): out (int64[pixels])
+ * receives the index of a cell of non-zero integral over the pixel, -1 when
+ * there is none.  Where several cells meet a pixel the reference keeps the one
+ * its threads wrote last; this keeps the largest index, so that the result
+ * does not depend on the order of the work.                                  */
+int sdot_get_image_of_cell_nums(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const int64_t *nb_pixels,
+                                int64_t *out, int mem_space);
+
 /* ---- Newton on the weights -------------------------------------------------
  * Replaces OptimalTransportSolver::solve( positions, weights, n, masses, rf )
  * (OptimalTransportSolver.tcc:27-119) and its sparse direct solve

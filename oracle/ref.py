@@ -66,6 +66,8 @@ def load():
         "ref_neighbors": (I64, [P]),
         "ref_neighbors_copy": (None, [P, P, P]),
         "ref_timings": (None, [P, P]),
+        "ref_get_image_integrals": (None, [P, P, P, P, P]),
+        "ref_get_image_of_cell_nums": (None, [P, P, P, P, P]),
     }
     for k, (r, a) in sig.items():
         f = getattr(L, k)
@@ -132,13 +134,17 @@ class RefPowerDiagram:
     def domain_measure(self):
         return self.L.ref_domain_measure(self.h)
 
-    def set_image_density(self, image, min_pt=None, max_pt=None):
+    def set_image_density(self, image, min_pt=None, max_pt=None, nb_coeffs=None):
+        """image: (ny, nx) values, or (6, ny, nx) coefficient planes (nb_coeffs = 6)."""
         img = _f(image)
-        sizes = np.array(img.shape[::-1], dtype=np.int64)
+        if nb_coeffs is None:
+            nb_coeffs = img.shape[0] if img.ndim == self.dim + 1 else 1
+        spatial = img.shape[1:] if nb_coeffs > 1 else img.shape
+        sizes = np.array(spatial[::-1], dtype=np.int64)
         mn = _f(min_pt if min_pt is not None else np.zeros(self.dim))
         mx = _f(max_pt if max_pt is not None else np.ones(self.dim))
         self._img = img
-        self.L.ref_set_image(self.h, _p(mn), _p(mx), _p(img), _p(sizes), 1)
+        self.L.ref_set_image(self.h, _p(mn), _p(mx), _p(img), _p(sizes), int(nb_coeffs))
 
     def update(self):
         self.L.ref_update(self.h)
@@ -180,6 +186,24 @@ class RefPowerDiagram:
         ids = np.zeros(cnt, dtype=np.int64)
         self.L.ref_neighbors_copy(self.h, _p(off), _p(ids))
         return off, ids
+
+    def image_integrals(self, min_pt, max_pt, nb_pixels):
+        """get_image_integrals: (ny, nx, 3) per pixel (sum m x, sum m y, sum m)."""
+        self._ensure()
+        mn, mx = _f(min_pt), _f(max_pt)
+        nbp = np.array(nb_pixels, dtype=np.int64)
+        out = np.zeros((int(nbp[1]), int(nbp[0]), 3))
+        self.L.ref_get_image_integrals(self.h, _p(mn), _p(mx), _p(nbp), _p(out))
+        return out
+
+    def image_of_cell_nums(self, min_pt, max_pt, nb_pixels):
+        """get_image_of_cell_nums: (ny, nx) int64, -1 where no cell."""
+        self._ensure()
+        mn, mx = _f(min_pt), _f(max_pt)
+        nbp = np.array(nb_pixels, dtype=np.int64)
+        out = np.zeros((int(nbp[1]), int(nbp[0])), dtype=np.int64)
+        self.L.ref_get_image_of_cell_nums(self.h, _p(mn), _p(mx), _p(nbp), _p(out))
+        return out
 
     def timings(self):
         t = np.zeros(4)

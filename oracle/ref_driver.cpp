@@ -26,6 +26,8 @@
 #include "src/sdot/PowerDiagram/get_integrals.h"
 #include "src/sdot/PowerDiagram/get_centroids.h"
 #include "src/sdot/PowerDiagram/get_der_integrals_wrt_weights.h"
+#include "src/sdot/PowerDiagram/get_image_integrals.h"
+#include "src/sdot/PowerDiagram/get_image_of_cell_nums.h"
 #include "src/sdot/Domains/ConvexPolyhedronAssembly.h"
 #include "src/sdot/Domains/ScaledImage.h"
 #include "src/sdot/Integration/Unit.h"
@@ -202,6 +204,26 @@ struct Ctx : CtxBase {
         return err;
     }
 
+    // get_image_integrals (get_image_integrals.h:16-78) and
+    // get_image_of_cell_nums (get_image_of_cell_nums.h:13-80), 2D
+    void image_integrals(const double *lo, const double *hi, const std::int64_t *nbp, double *out, bool nums,
+                         std::int64_t *out_nums) {
+        if constexpr (dim == 2) {
+            Pt a, b;
+            std::array<std::size_t, dim> s;
+            for (int d = 0; d < dim; ++d) { a[d] = lo[d]; b[d] = hi[d]; s[d] = std::size_t(nbp[d]); }
+            with_bounds_and_rf([&](auto &bounds, auto rf) {
+                if (nums) {
+                    std::vector<std::size_t> r(s[0] * s[1]);
+                    get_image_of_cell_nums(r.data(), grid, bounds, pos.data(), w.data(), w.size(), rf, a, b, s);
+                    for (std::size_t i = 0; i < r.size(); ++i) out_nums[i] = std::int64_t(r[i]);
+                } else {
+                    get_image_integrals(out, grid, bounds, pos.data(), w.data(), w.size(), rf, a, b, s);
+                }
+            });
+        }
+    }
+
     // cut ids of the final cell boundary (before any bounds intersection),
     // one list per Dirac: what the traversal hands to the callback.
     void neighbors() {
@@ -309,6 +331,13 @@ void ref_set_image(void *h, const double *min_pt, const double *max_pt, const do
 }
 
 void ref_update(void *h) { dispatch(h, [&](auto &c) { c.update(); return 0; }); }
+void ref_get_image_integrals(void *h, const double *lo, const double *hi, const std::int64_t *nbp, double *out) {
+    dispatch(h, [&](auto &c) { c.image_integrals(lo, hi, nbp, out, false, nullptr); return 0; });
+}
+void ref_get_image_of_cell_nums(void *h, const double *lo, const double *hi, const std::int64_t *nbp,
+                                std::int64_t *out) {
+    dispatch(h, [&](auto &c) { c.image_integrals(lo, hi, nbp, nullptr, true, out); return 0; });
+}
 void ref_get_integrals(void *h, double *out) { dispatch(h, [&](auto &c) { c.integrals(out); return 0; }); }
 void ref_get_centroids(void *h, double *out_c, double *out_m) {
     dispatch(h, [&](auto &c) { c.centroids(out_c, out_m); return 0; });

@@ -516,6 +516,34 @@ double or_poly_integrate_poly6(const or_poly *p, const double *c) {
     return res;
 }
 
+static double poly6_at(const double *c, double x, double y) {
+    return c[0] + c[1] * x + c[2] * y + c[3] * x * x + c[4] * x * y + c[5] * y * y;
+}
+
+/* first moments (integrals of x f and y f) of the same density over the fan
+ * triangles, by the 7-point triangle rule (weights 1/20 at the vertices, 2/15
+ * at the edge midpoints, 9/20 at the centroid, times the area), exact for
+ * cubics: the quantity of add_centroid_contrib( Polynomial<6>, Unit )
+ * (ConvexPolyhedron2.tcc:980-1044) */
+static void poly6_moments(const or_poly *p, const double *c, double *mom) {
+    for (int i = 2; i < p->n; ++i) {
+        double v[3][2] = {{p->x[0], p->y[0]}, {p->x[i - 1], p->y[i - 1]}, {p->x[i], p->y[i]}};
+        double a = 0.5 * (v[0][0] * (v[1][1] - v[2][1]) + v[1][0] * (v[2][1] - v[0][1]) + v[2][0] * (v[0][1] - v[1][1]));
+        double sx = 0, sy = 0;
+        for (int k = 0; k < 3; ++k) {
+            double fv = poly6_at(c, v[k][0], v[k][1]);
+            double mx = 0.5 * (v[k][0] + v[(k + 1) % 3][0]), my = 0.5 * (v[k][1] + v[(k + 1) % 3][1]);
+            double fm = poly6_at(c, mx, my);
+            sx += (1.0 / 20.0) * v[k][0] * fv + (2.0 / 15.0) * mx * fm;
+            sy += (1.0 / 20.0) * v[k][1] * fv + (2.0 / 15.0) * my * fm;
+        }
+        double gx = (v[0][0] + v[1][0] + v[2][0]) / 3, gy = (v[0][1] + v[1][1] + v[2][1]) / 3;
+        double fg = poly6_at(c, gx, gy);
+        mom[0] += a * (sx + (9.0 / 20.0) * gx * fg);
+        mom[1] += a * (sy + (9.0 / 20.0) * gy * fg);
+    }
+}
+
 static void min_max_position(const or_poly *p, double *mn, double *mx) {
     mn[0] = mn[1] = DBL_MAX;
     mx[0] = mx[1] = -DBL_MAX;
@@ -698,11 +726,14 @@ static void push_item(CellAcc *a, int64_t c, double v) {
  * with for_each_boundary_item( Constant, Unit ) (ConvexPolyhedron2.tcc:437-478) */
 static void piece(CellAcc *a, const or_poly *cp, int is_poly6, const double *c6, double coeff) {
     if (is_poly6) {
-        a->mass += or_poly_integrate_poly6(cp, c6);
-        return; /* the reference has no centroid / boundary for Polynomial<6> on the path */
+        const double m6 = or_poly_integrate_poly6(cp, c6);
+        a->mass += m6;
+        a->mass_c += m6;
+        poly6_moments(cp, c6, a->ctd);
+    } else {
+        a->mass += coeff * or_poly_measure(cp);
+        centroid_contrib(cp, coeff, a->ctd, &a->mass_c);
     }
-    a->mass += coeff * or_poly_measure(cp);
-    centroid_contrib(cp, coeff, a->ctd, &a->mass_c);
     const double x0 = a->pos[2 * a->i], y0 = a->pos[2 * a->i + 1];
     if (cp->n == 0) {
         if (cp->sr >= 0) {
@@ -719,6 +750,11 @@ static void piece(CellAcc *a, const or_poly *cp, int is_poly6, const double *c6,
         } else {
             double dx = cp->x[i1] - cp->x[i0], dy = cp->y[i1] - cp->y[i0];
             m = coeff * sqrt(dx * dx + dy * dy);
+            if (is_poly6) /* for_each_boundary_item( Polynomial<6>, Unit ) (:180-214): Simpson along the edge */
+                m = sqrt(dx * dx + dy * dy) / 6.0 *
+                    (poly6_at(c6, cp->x[i0], cp->y[i0]) +
+                     4.0 * poly6_at(c6, 0.5 * (cp->x[i0] + cp->x[i1]), 0.5 * (cp->y[i0] + cp->y[i1])) +
+                     poly6_at(c6, cp->x[i1], cp->y[i1]));
         }
         int64_t id = cp->id[i0];
         if (id == -1) continue;

@@ -75,6 +75,11 @@ struct HostPoly {
 
 const double kBoxNrm[4][2] = {{0, -1}, {1, 0}, {0, 1}, {-1, 0}};
 
+// Domain polygons of more than CAP_FAST_2D vertices start every cell in the
+// warp tier (polygons of up to CAP_HUGE_2D vertices); this leaves each cell
+// room for 64 bisector edges.
+constexpr int kMaxDomainVertices = CAP_HUGE_2D - 64;
+
 // ConvexPolyhedron2( Box ) (ConvexPolyhedron2.tcc:76-106)
 Item2 box_item(double x0, double y0, double x1, double y1, double coeff) {
     Item2 it;
@@ -190,6 +195,9 @@ struct sdot_ctx {
         dfree(cnt_orig); dfree(offsets); dfree(nb_offsets);
         dfree(ovf_list); dfree(ovf_list2); dfree(ovf_cnt2); dfree(ovf_list3); dfree(ovf_cnt3); dfree(hint3);
         dfree(dstat);
+        dfree(ras_buf);
+        dfree(ras_nums);
+        ras_cap = 0;
         ovf_cnt = nullptr;
         err = nullptr;
         guard = nullptr;
@@ -256,7 +264,7 @@ struct sdot_ctx {
     void upload_domain() {
         if (!dom_dirty) return;
         if (has_image) {
-            mode = DM_IMAGE;
+            mode = img_ncoeffs == 6 ? DM_IMAGE6 : DM_IMAGE;
             std::vector<double> st = {img_lo[0], img_lo[1], img_hi[0], img_lo[1], img_hi[0], img_hi[1], img_lo[0], img_hi[1]};
             start_n = 4;
             dalloc(d_start, 8);
@@ -297,8 +305,9 @@ struct sdot_ctx {
             item_nv = off.back();
             item_off_h = off;
             for (size_t k = 0; k + 1 < off.size(); ++k)
-                if (off[k + 1] - off[k] > CAP_FAST_2D)
-                    throw Unsupported("a domain shape has more vertices than the cell capacity");
+                if (off[k + 1] - off[k] > kMaxDomainVertices)
+                    throw Unsupported("a domain shape has more than " + std::to_string(kMaxDomainVertices) +
+                                      " vertices");
             dalloc(d_item_off, off.size());
             SDOT_CUDA(cudaMemcpyAsync(d_item_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
             dalloc(d_item_xy, xy.size());
@@ -310,7 +319,8 @@ struct sdot_ctx {
         } else {
             throw BadArg("no domain: call sdot_add_box_shape (or another add_..._shape) first");
         }
-        if (start_n > CAP_FAST_2D) throw Unsupported("domain polygon has more vertices than the cell capacity");
+        if (start_n > kMaxDomainVertices)
+            throw Unsupported("the domain polygon has more than " + std::to_string(kMaxDomainVertices) + " vertices");
         dom_dirty = false;
     }
 
@@ -354,6 +364,9 @@ struct sdot_ctx {
             if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
             return;
         }
+        if (has_image && img_ncoeffs == 6 && ball)
+            throw Unsupported("no ball cut with a piecewise-quadratic image (the reference's Polynomial<6> arc "
+                              "integrals are a TODO)");
         upload_domain();
     }
 
@@ -583,6 +596,66 @@ struct sdot_ctx {
         SDOT_CUDA(cudaMemcpyAsync(&nb_total, nb_offsets + n, sizeof(long long), cudaMemcpyDeviceToHost, stream));
         SDOT_CUDA(cudaStreamSynchronize(stream));
         nb_dirty = false;
+    }
+
+    // get_image_integrals / get_image_of_cell_nums (get_image_integrals.h:16-78,
+    // get_image_of_cell_nums.h:13-80): every cell (each piece cell ∩ shape
+    // with its density, or cell ∩ disc) integrated over the pixels of the
+    // raster [lo, hi] of nx x ny pixels; results in ras_buf (device, nx * ny *
+    // 3 doubles) or ras_nums (device, nx * ny int64)
+    double *ras_buf = nullptr;
+    long long *ras_nums = nullptr;
+    long long ras_cap = 0;
+    void rasterize(const double *lo, const double *hi, long long nx, long long ny, bool nums) {
+        if (dim != 2) throw Unsupported("image integrals are available in 2D");
+        if (nx <= 0 || ny <= 0 || nx * ny > (1LL << 31)) throw BadArg("bad raster size");
+        if (!(hi[0] > lo[0]) || !(hi[1] > lo[1])) throw BadArg("bad raster corners");
+        check_domain();
+        if (mode == DM_IMAGE || mode == DM_IMAGE6)
+            throw Unsupported("image integrals over an image density are not available in this build");
+        reserve_eval();
+        ensure_tree();
+        const long long np = nx * ny;
+        if (ras_cap < np) {
+            dalloc(ras_buf, size_t(3 * np));
+            dalloc(ras_nums, size_t(np));
+            ras_cap = np;
+        }
+        if (nums)
+            SDOT_CUDA(cudaMemsetAsync(ras_nums, 0xff, size_t(np) * sizeof(long long), stream));  // -1
+        else
+            SDOT_CUDA(cudaMemsetAsync(ras_buf, 0, size_t(3 * np) * sizeof(double), stream));
+        SDOT_CUDA(cudaMemsetAsync(dstat, 0, sizeof(DevStatus), stream));
+        Cell2DArgs a = args();
+        a.mixed = 0;
+        a.ras = nums ? nullptr : ras_buf;
+        a.ras_nums = nums ? ras_nums : nullptr;
+        a.perm = perm();
+        for (int d = 0; d < 2; ++d) {
+            a.ras_lo[d] = lo[d];
+            a.ras_hi[d] = hi[d];
+        }
+        a.ras_nx = int(nx);
+        a.ras_ny = int(ny);
+        if (mode == DM_MULTI) {
+            // one pass per shape, with the shape as the starting polygon and
+            // its density (the pieces of ConvexPolyhedronAssembly::for_each_intersection)
+            for (size_t k = 0; k + 1 < item_off_h.size(); ++k) {
+                Cell2DArgs b = a;
+                b.mode = DM_RASTER;
+                b.start_n = item_off_h[k + 1] - item_off_h[k];
+                b.start_xy = d_item_xy + 2 * item_off_h[k];
+                b.coeff = items[k].coeff;
+                cells2d_launch(b, scratch, stream);
+            }
+        } else {
+            a.mode = DM_RASTER;
+            cells2d_launch(a, scratch, stream);
+        }
+        SDOT_CUDA(cudaMemcpyAsync(hstat, dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+        SDOT_CUDA(cudaStreamSynchronize(stream));
+        last_err = hstat->err;
+        for (int k = 0; k < 3; ++k) last_guard[k] = hstat->guard[k];
     }
 
     void copy_out(void *dst, const void *src, size_t bytes, int mem_space) {
@@ -994,7 +1067,8 @@ int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *ma
     return guarded(ctx, [&] {
         if (!min_pt || !max_pt || !data || !sizes) throw BadArg("null image argument");
         if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
-        if (nb_coeffs != 1) throw Unsupported("only piecewise-constant images (nb_coeffs = 1) are available");
+        if (nb_coeffs != 1 && nb_coeffs != 6)
+            throw Unsupported("images have nb_coeffs = 1 (piecewise constant) or 6 (piecewise quadratic)");
         if (sizes[0] <= 0 || sizes[1] <= 0) throw BadArg("bad image size");
         ctx->items.clear();
         ctx->has_image = true;
@@ -1041,10 +1115,29 @@ int sdot_clear_domain(sdot_ctx *ctx) {
 
 static double domain_measure(const sdot_ctx *ctx) {
     if (ctx->has_image) {
-        // ScaledImage::measure (ScaledImage.tcc:36-69), nb_coeffs == 1: mean * volume
+        // ScaledImage::measure (ScaledImage.tcc:36-69): the mean over the
+        // pixels of the density's average on the pixel, times the area
+        const long long nx = ctx->img_size[0], ny = ctx->img_size[1], np = nx * ny;
         double s = 0;
-        for (double v : ctx->img_data) s += v;
-        s /= double(ctx->img_data.size());
+        if (ctx->img_ncoeffs == 6) {
+            // average of c0 + c1 x + c2 y + c3 x^2 + c4 xy + c5 y^2 on a pixel
+            // of centre (cx, cy) and size dx x dy: the value at the centre
+            // plus (c3 dx^2 + c5 dy^2) / 12
+            const double dx = (ctx->img_hi[0] - ctx->img_lo[0]) / double(nx);
+            const double dy = (ctx->img_hi[1] - ctx->img_lo[1]) / double(ny);
+            const double *c = ctx->img_data.data();
+            for (long long yi = 0, o = 0; yi < ny; ++yi)
+                for (long long xi = 0; xi < nx; ++xi, ++o) {
+                    const double cx = ctx->img_lo[0] + dx * double(xi) + 0.5 * dx;
+                    const double cy = ctx->img_lo[1] + dy * double(yi) + 0.5 * dy;
+                    s += c[o] + c[np + o] * cx + c[2 * np + o] * cy + c[3 * np + o] * cx * cx +
+                         c[4 * np + o] * cx * cy + c[5 * np + o] * cy * cy +
+                         (1.0 / 12.0) * (c[3 * np + o] * dx * dx + c[5 * np + o] * dy * dy);
+                }
+        } else {
+            for (double v : ctx->img_data) s += v;
+        }
+        s /= double(np);
         for (int d = 0; d < 2; ++d) s *= ctx->img_hi[d] - ctx->img_lo[d];
         return s;
     }
@@ -1188,6 +1281,28 @@ int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *c
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
         *count_inout = tot;
         return int(SDOT_OK);
+    });
+}
+
+int sdot_get_image_integrals(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const int64_t *nb_pixels,
+                             double *out, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!min_pt || !max_pt || !nb_pixels || !out) throw BadArg("null argument");
+        ctx->rasterize(min_pt, max_pt, nb_pixels[0], nb_pixels[1], false);
+        ctx->copy_out(out, ctx->ras_buf, size_t(3 * nb_pixels[0] * nb_pixels[1]) * sizeof(double), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return ctx->finish_status();
+    });
+}
+
+int sdot_get_image_of_cell_nums(sdot_ctx *ctx, const double *min_pt, const double *max_pt, const int64_t *nb_pixels,
+                                int64_t *out, int mem_space) {
+    return guarded(ctx, [&] {
+        if (!min_pt || !max_pt || !nb_pixels || !out) throw BadArg("null argument");
+        ctx->rasterize(min_pt, max_pt, nb_pixels[0], nb_pixels[1], true);
+        ctx->copy_out(out, ctx->ras_nums, size_t(nb_pixels[0] * nb_pixels[1]) * sizeof(int64_t), mem_space);
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return ctx->finish_status();
     });
 }
 

@@ -76,8 +76,17 @@ struct Out {
 
 // Integrates a streamed polygon (one piece at a time) and collects the
 // boundary measures for the Hessian row.  P: the cell's polygon view (its
-// ids name the neighbours).
-template <bool DIRECT, class P = PolyView<double>>
+// ids name the neighbours).  POLY: the density of a piece is the quadratic
+// c0 + c1 x + c2 y + c3 x^2 + c4 x y + c5 y^2 (absolute coordinates) of a
+// piecewise-quadratic image (ScaledImage with nb_coeffs = 6), integrated
+// exactly: the edge-midpoint rule on each fan triangle for the mass (exact
+// for quadratics), the 7-point rule (vertices 1/20, edge midpoints 2/15,
+// centroid 9/20 of the area; exact for cubics) for the first moments, and
+// Simpson's rule along each edge for the boundary measures (exact for
+// quadratics).  The reference evaluates the same integrals from expanded
+// closed forms (ConvexPolyhedron2.tcc:2181-2225 integration, :980-1044
+// add_centroid_contrib, :180-214 for_each_boundary_item).
+template <bool DIRECT, class P = PolyView<double>, bool POLY = false>
 struct Sink {
     const P &cell;
     const double *pos;
@@ -102,11 +111,21 @@ struct Sink {
                   Out &ro)
         : cell(c), pos(p), c0x(x0), c0y(y0), sqw0(sw), cx(x0), cy(y0), r(r_), acc(a), acc_st(ast), row(ro) {}
 
+    double q[6] = {0, 0, 0, 0, 0, 0};  // POLY: the piece's density coefficients
+
     SDOT_HDI void begin_piece(double c) {
         coeff = c;
         has_first = false;
         cnt = 0;
         tr2 = arcs = pm = pcx = pcy = 0;
+    }
+    // POLY: the coefficients of pixel p, plane k at c[p + k * plane]
+    SDOT_HDI void begin_piece_poly(const double *c, long long plane) {
+        for (int k = 0; k < 6; ++k) q[k] = c[k * plane];
+        begin_piece(1.0);
+    }
+    SDOT_HDI double f(double x, double y) const {
+        return q[0] + q[1] * x + q[2] * y + q[3] * x * x + q[4] * x * y + q[5] * y * y;
     }
     SDOT_HDI void line(int t, double len) {
         if (t < 0) return;
@@ -135,7 +154,11 @@ struct Sink {
             der0 += 0.5 * (coeff * (a1 - a0) * r) / sqw0;
         } else {
             const double dx = bx - ax, dy = by - ay;
-            line(t, sqrt(dx * dx + dy * dy));
+            const double len = sqrt(dx * dx + dy * dy);
+            if (POLY)  // Simpson along the edge; line() multiplies by coeff = 1
+                line(t, len * (1.0 / 6.0) * (f(ax, ay) + 4.0 * f(0.5 * (ax + bx), 0.5 * (ay + by)) + f(bx, by)));
+            else
+                line(t, len);
         }
     }
     SDOT_HDI void push(double x, double y, int tag) {
@@ -148,11 +171,25 @@ struct Sink {
         if (++cnt >= 3) {
             const double t2 = fx * (py - y) + px * (y - fy) + x * (fy - py);
             tr2 += t2;
-            const double lea = 0.5 * t2 * coeff;
-            const double f = (1.0 / 3.0) * lea;
-            pcx += f * (fx + px + x);
-            pcy += f * (fy + py + y);
-            pm += lea;
+            if (POLY) {
+                const double a = 0.5 * t2;
+                const double m1x = 0.5 * (fx + px), m1y = 0.5 * (fy + py), m2x = 0.5 * (px + x), m2y = 0.5 * (py + y);
+                const double m3x = 0.5 * (x + fx), m3y = 0.5 * (y + fy);
+                const double gx = (1.0 / 3.0) * (fx + px + x), gy = (1.0 / 3.0) * (fy + py + y);
+                const double f1 = f(m1x, m1y), f2 = f(m2x, m2y), f3 = f(m3x, m3y);
+                const double fa = f(fx, fy), fb = f(px, py), fc = f(x, y), fg = f(gx, gy);
+                pm += a * (1.0 / 3.0) * (f1 + f2 + f3);
+                pcx += a * ((1.0 / 20.0) * (fx * fa + px * fb + x * fc) +
+                            (2.0 / 15.0) * (m1x * f1 + m2x * f2 + m3x * f3) + (9.0 / 20.0) * gx * fg);
+                pcy += a * ((1.0 / 20.0) * (fy * fa + py * fb + y * fc) +
+                            (2.0 / 15.0) * (m1y * f1 + m2y * f2 + m3y * f3) + (9.0 / 20.0) * gy * fg);
+            } else {
+                const double lea = 0.5 * t2 * coeff;
+                const double f = (1.0 / 3.0) * lea;
+                pcx += f * (fx + px + x);
+                pcy += f * (fy + py + y);
+                pm += lea;
+            }
         }
         px = x; py = y; pt = tag;
     }
@@ -173,12 +210,117 @@ struct Sink {
             }
             return;
         }
-        mass += coeff * (tr2 * 0.5 + arcs);
+        mass += POLY ? pm : coeff * (tr2 * 0.5 + arcs);
         mass_c += pm;
         momx += pcx;
         momy += pcy;
     }
 };
+
+// Area of a streamed (clipped) polygon, segments of the clipping disc
+// included (fan from the first vertex plus the arc segments, as Sink).
+struct AreaSink {
+    double cx, cy, r;
+    bool has_first = false;
+    double fx = 0, fy = 0, px = 0, py = 0;
+    int pt = 0, cnt = 0;
+    double tr2 = 0, arcs = 0;
+    SDOT_HDI AreaSink(double x, double y, double rr) : cx(x), cy(y), r(rr) {}
+    SDOT_HDI void edge(double ax, double ay, int t, double bx, double by) {
+        if (t == ID_ARC) arcs += arc_area(ax, ay, bx, by, cx, cy, r);
+    }
+    SDOT_HDI void push(double x, double y, int tag) {
+        if (!has_first) {
+            has_first = true;
+            fx = x;
+            fy = y;
+        } else {
+            edge(px, py, pt, x, y);
+        }
+        if (++cnt >= 3) tr2 += fx * (py - y) + px * (y - fy) + x * (fy - py);
+        px = x;
+        py = y;
+        pt = tag;
+    }
+    SDOT_HDI void finish() {
+        if (has_first) edge(px, py, pt, fx, fy);
+    }
+    // radius: the disc radius after clipping (> 0 keeps a vertex-free piece
+    // as the full disc), or -1 when there is no disc
+    SDOT_HDI double area(double radius) const {
+        if (cnt == 0) return radius > 0 ? kPi * radius * radius : 0.0;
+        return 0.5 * tr2 + arcs;
+    }
+};
+
+// Integrates the cell of sorted Dirac s (its polygon before disc clipping,
+// n vertices) over the pixels of the raster that its bounding box meets:
+// get_image_integrals / get_image_of_cell_nums
+// (get_image_integrals.h:16-78, get_image_of_cell_nums.h:13-80) clip each
+// pixel box by the cell and integrate; here the cell is clipped by the pixel's
+// four lines (and the disc), the same convex set.
+template <bool BALL, class P>
+SDOT_KFN void raster_cell(const Cell2DArgs &A, long long s, const P &cell, int n, double c0x, double c0y,
+                          double r) {
+    if (n <= 0) return;
+    double xmin = cell.X(0), xmax = xmin, ymin = cell.Y(0), ymax = ymin;
+    for (int k = 1; k < n; ++k) {
+        xmin = fmin(xmin, cell.X(k)); xmax = fmax(xmax, cell.X(k));
+        ymin = fmin(ymin, cell.Y(k)); ymax = fmax(ymax, cell.Y(k));
+    }
+    if (BALL) {
+        xmin = fmax(xmin, c0x - r); xmax = fmin(xmax, c0x + r);
+        ymin = fmax(ymin, c0y - r); ymax = fmin(ymax, c0y + r);
+    }
+    const double psx = (A.ras_hi[0] - A.ras_lo[0]) / A.ras_nx, psy = (A.ras_hi[1] - A.ras_lo[1]) / A.ras_ny;
+    const double fx0 = floor((xmin - A.ras_lo[0]) / psx), fx1 = floor((xmax - A.ras_lo[0]) / psx);
+    const double fy0 = floor((ymin - A.ras_lo[1]) / psy), fy1 = floor((ymax - A.ras_lo[1]) / psy);
+    if (!(fx1 >= 0 && fy1 >= 0 && fx0 < A.ras_nx && fy0 < A.ras_ny)) return;  // outside the raster (or NaN)
+    const int ix0 = int(fmax(fx0, 0.0)), ix1 = int(fmin(fx1, double(A.ras_nx - 1)));
+    const int iy0 = int(fmax(fy0, 0.0)), iy1 = int(fmin(fy1, double(A.ras_ny - 1)));
+    const long long orig = A.perm ? A.perm[s] : s;
+    for (int iy = iy0; iy <= iy1; ++iy) {
+        const double y0 = A.ras_lo[1] + psy * double(iy), y1 = A.ras_lo[1] + psy * double(iy + 1);
+        for (int ix = ix0; ix <= ix1; ++ix) {
+            const double x0 = A.ras_lo[0] + psx * double(ix), x1 = A.ras_lo[0] + psx * double(ix + 1);
+            AreaSink as(c0x, c0y, r);
+            double m;
+            if (BALL) {
+                DiscClip<AreaSink> dc(as, c0x, c0y, r);
+                AxisClip<DiscClip<AreaSink>> c4(dc, 1, y1, -1.0, PID_OWN);
+                AxisClip<AxisClip<DiscClip<AreaSink>>> c3(c4, 1, y0, 1.0, PID_OWN);
+                AxisClip<AxisClip<AxisClip<DiscClip<AreaSink>>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                AxisClip<AxisClip<AxisClip<AxisClip<DiscClip<AreaSink>>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                stream_cell(cell, n, c1);
+                m = A.coeff * as.area(dc.result_radius());
+            } else {
+                AxisClip<AreaSink> c4(as, 1, y1, -1.0, PID_OWN);
+                AxisClip<AxisClip<AreaSink>> c3(c4, 1, y0, 1.0, PID_OWN);
+                AxisClip<AxisClip<AxisClip<AreaSink>>> c2(c3, 0, x1, -1.0, PID_OWN);
+                AxisClip<AxisClip<AxisClip<AxisClip<AreaSink>>>> c1(c2, 0, x0, 1.0, PID_OWN);
+                stream_cell(cell, n, c1);
+                m = A.coeff * as.area(-1.0);
+            }
+            if (m == 0) continue;
+            const long long pix = (long long)iy * A.ras_nx + ix;
+#ifdef __CUDA_ARCH__
+            if (A.ras) {
+                atomicAdd(&A.ras[3 * pix], m * c0x);
+                atomicAdd(&A.ras[3 * pix + 1], m * c0y);
+                atomicAdd(&A.ras[3 * pix + 2], m);
+            }
+            if (A.ras_nums) atomicMax(&A.ras_nums[pix], orig);
+#else
+            if (A.ras) {
+                A.ras[3 * pix] += m * c0x;
+                A.ras[3 * pix + 1] += m * c0y;
+                A.ras[3 * pix + 2] += m;
+            }
+            if (A.ras_nums && A.ras_nums[pix] < orig) A.ras_nums[pix] = orig;
+#endif
+        }
+    }
+}
 
 // Records the ids of the streamed (disc-clipped) cell boundary.
 template <class P = PolyView<double>>
@@ -643,8 +785,12 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
     if (n < 0) return false;
 
     const double r = BALL ? sqrt(w0) : -1.0;
+    if (MODE == DM_RASTER) {
+        raster_cell<BALL>(A, s, cell, n, c0x, c0y, r);
+        return true;
+    }
     constexpr bool DIRECT = MODE == DM_SINGLE;
-    using SinkT = Sink<DIRECT, P>;
+    using SinkT = Sink<DIRECT, P, MODE == DM_IMAGE6>;
     SinkT sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
     sink.n_diracs = A.n;
 
@@ -676,7 +822,7 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
     } else {
         for (int k = 0; k < n; ++k) acc[k * acc_st] = -1.0;
         if (n > 0) {
-            if (MODE == DM_IMAGE) {
+            if (MODE == DM_IMAGE || MODE == DM_IMAGE6) {
                 double xmin = cell.X(0), xmax = xmin, ymin = cell.Y(0), ymax = ymin;
                 for (int k = 1; k < n; ++k) {
                     xmin = fmin(xmin, cell.X(k)); xmax = fmax(xmax, cell.X(k));
@@ -697,8 +843,12 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
                     const double y0 = A.img_lo[1] + psy * double(iy), y1 = A.img_lo[1] + psy * double(iy + 1);
                     for (int ix = ix0; ix <= ix1; ++ix) {
                         const double x0 = A.img_lo[0] + psx * double(ix), x1 = A.img_lo[0] + psx * double(ix + 1);
-                        sink.begin_piece(A.img[(long long)iy * A.img_nx + ix]);
-                        if (BALL) {
+                        if (MODE == DM_IMAGE6)
+                            sink.begin_piece_poly(A.img + (long long)iy * A.img_nx + ix,
+                                                  (long long)A.img_nx * A.img_ny);
+                        else
+                            sink.begin_piece(A.img[(long long)iy * A.img_nx + ix]);
+                        if (BALL && MODE == DM_IMAGE) {
                             DiscClip<SinkT> dc(sink, c0x, c0y, r);
                             AxisClip<DiscClip<SinkT>> c4(dc, 1, y1, -1.0, PID_OWN);
                             AxisClip<AxisClip<DiscClip<SinkT>>> c3(c4, 1, y0, 1.0, PID_OWN);
@@ -777,7 +927,7 @@ __device__ void push_overflow(const Cell2DArgs &A, long long s) {
 // thread beyond the polygon: the per-edge accumulators of the image mode
 template <int MODE>
 constexpr int smem_extra_halves() {
-    return MODE == DM_IMAGE ? 2 : 0;
+    return MODE == DM_IMAGE || MODE == DM_IMAGE6 ? 2 : 0;
 }
 
 template <int MODE, bool BALL>
@@ -1042,6 +1192,14 @@ void launch_fast(const Cell2DArgs &a, int bs, cudaStream_t st) {
     SDOT_CUDA(cudaGetLastError());
 }
 
+// Every cell into the warp tier's list (domain polygons larger than the fast
+// tier's polygons).
+__global__ void k_all_cells(int *list, int *cnt, long long n) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s < n) list[s] = int(s);
+    if (s == 0) *cnt = int(n);
+}
+
 // Counters the fast kernel appends to: zeroed before every launch of it.
 void reset_overflow(const Cell2DArgs &a, cudaStream_t st) {
     SDOT_CUDA(cudaMemsetAsync(a.ovf_cnt, 0, sizeof(int), st));
@@ -1058,6 +1216,18 @@ void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
         SDOT_CUDA(cudaFuncSetAttribute(k_cells2d_mixed<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(fast_smem<MODE, BALL>(T2D_MAX, true))));
     });
+    if (a.start_n > CAP_FAST_2D) {
+        // the starting polygon alone overflows the fast tier: every cell is
+        // built by the warp tier (polygons of up to CAP_HUGE_2D vertices)
+        reset_overflow(a, st);
+        k_all_cells<<<ceil_div(a.n, 256), 256, 0, st>>>(a.ovf_list, a.ovf_cnt, a.n);
+        note_launch();
+        k_cells2d_wtier<MODE, BALL><<<WTIER_WARPS / 4, 128, 0, st>>>(a, static_cast<double *>(scratch), WTIER_WARPS,
+                                                                      a.ovf_list, a.ovf_cnt);
+        note_launch();
+        SDOT_CUDA(cudaGetLastError());
+        return;
+    }
     static PerDevice<int> tuned[2];  // best block size per device: FP64, mixed
     PerDevice<int> &tu = tuned[a.mixed ? 1 : 0];
     int best = tu.get();
@@ -1116,6 +1286,12 @@ void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
         if (ball) launch_all<DM_SINGLE, true>(a, scratch, st); else launch_all<DM_SINGLE, false>(a, scratch, st);
     } else if (a.mode == DM_IMAGE) {
         if (ball) launch_all<DM_IMAGE, true>(a, scratch, st); else launch_all<DM_IMAGE, false>(a, scratch, st);
+    } else if (a.mode == DM_RASTER) {
+        if (ball) launch_all<DM_RASTER, true>(a, scratch, st); else launch_all<DM_RASTER, false>(a, scratch, st);
+    } else if (a.mode == DM_IMAGE6) {
+        // the reference integrates no piecewise-quadratic density over disc arcs
+        if (ball) throw CudaError{cudaErrorInvalidValue, "cells2d_launch: no disc clip with nb_coeffs = 6"};
+        launch_all<DM_IMAGE6, false>(a, scratch, st);
     } else {
         throw CudaError{cudaErrorInvalidValue, "cells2d_launch: a domain of several shapes runs one pass per shape"};
     }

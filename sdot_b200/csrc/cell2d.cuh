@@ -5,7 +5,12 @@
 
 namespace sdot {
 
-enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2 };
+// DM_IMAGE: piecewise-constant image (nb_coeffs = 1); DM_IMAGE6: piecewise
+// quadratic (nb_coeffs = 6, planes of img_nx * img_ny coefficients)
+// DM_RASTER: no cell outputs; each cell (with the starting shape's density)
+// is integrated over the pixels of a raster (get_image_integrals,
+// get_image_of_cell_nums)
+enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2, DM_IMAGE6 = 3, DM_RASTER = 4 };
 
 // Cell polygon capacities of the two tiers.  Every cell is first built by
 // the fast kernel (one thread per cell, polygon in shared memory); cells that
@@ -77,6 +82,15 @@ struct Cell2DArgs {
     // cells that overflow the fast tier (sorted indices handed to the warp tier)
     int *ovf_list = nullptr;
     int *ovf_cnt = nullptr;
+    // raster outputs (DM_RASTER): per pixel (x-fastest) the sums of m x_i,
+    // m y_i and m over the cells i, m the integral of cell i over the pixel
+    // (ras, 3 doubles per pixel), and the largest caller index of a cell of
+    // non-zero integral over the pixel (ras_nums, -1 if none)
+    double *ras = nullptr;
+    long long *ras_nums = nullptr;
+    double ras_lo[2] = {0, 0}, ras_hi[2] = {1, 1};
+    int ras_nx = 0, ras_ny = 0;
+    const int *perm = nullptr;     // sorted -> caller index
     unsigned *err = nullptr;
     int *guard = nullptr;          // first failed guard: (code, sorted index, value)
     long long item_nv = 0;         // number of item vertices (multi items)

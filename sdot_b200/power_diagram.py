@@ -109,13 +109,21 @@ class PowerDiagram:
         pts = _f64(points, (self.dim + 1, self.dim))
         self._check(self._lib.sdot_add_simplex_shape(self._ctx, _ptr(pts), float(coeff)))
 
-    def set_image_density(self, image, min_pt=None, max_pt=None):
-        """image: numpy array of shape (ny, nx) (last axis is x)."""
+    def set_image_density(self, image, min_pt=None, max_pt=None, nb_coeffs=None):
+        """image: numpy array of shape (ny, nx) (last axis is x) for a
+        piecewise-constant density, or (6, ny, nx) for a piecewise-quadratic
+        one (nb_coeffs = 6: per pixel c0 + c1 x + c2 y + c3 x^2 + c4 x y +
+        c5 y^2 in absolute coordinates, plane k holding c_k; the layout of
+        ScaledImage's data)."""
         img = _f64(image)
-        sizes = np.array(img.shape[::-1], dtype=np.int64)
+        if nb_coeffs is None:
+            nb_coeffs = img.shape[0] if img.ndim == self.dim + 1 else 1
+        spatial = img.shape[1:] if nb_coeffs > 1 else img.shape
+        sizes = np.array(spatial[::-1], dtype=np.int64)
         mn = _f64(min_pt if min_pt is not None else np.zeros(self.dim))
         mx = _f64(max_pt if max_pt is not None else np.ones(self.dim))
-        self._check(self._lib.sdot_set_image_density(self._ctx, _ptr(mn), _ptr(mx), _ptr(img), _ptr(sizes), 1))
+        self._check(self._lib.sdot_set_image_density(self._ctx, _ptr(mn), _ptr(mx), _ptr(img), _ptr(sizes),
+                                                     int(nb_coeffs)))
 
     def set_polynomial_density(self, coeffs):
         """3D: multiplies the domain's density by c0 + c1 x + c2 y + c3 z +
@@ -181,6 +189,28 @@ class PowerDiagram:
         self._check(self._lib.sdot_get_neighbors(self._ctx, _ptr(offsets), _ptr(ids), ctypes.byref(cnt),
                                                  SDOT_HOST))
         return offsets, ids
+
+    def image_integrals(self, min_pt, max_pt, nb_pixels):
+        """get_image_integrals: for the raster of nb_pixels = (nx, ny) pixels
+        over [min_pt, max_pt], an array (ny, nx, 3) holding per pixel
+        (sum m_i x_i, sum m_i y_i, sum m_i), m_i the integral of cell i over
+        the pixel."""
+        mn, mx = _f64(min_pt), _f64(max_pt)
+        nbp = np.array(nb_pixels, dtype=np.int64)
+        out = np.empty((int(nbp[1]), int(nbp[0]), 3))
+        self._check(self._lib.sdot_get_image_integrals(self._ctx, _ptr(mn), _ptr(mx), _ptr(nbp), _ptr(out), SDOT_HOST))
+        return out
+
+    def image_of_cell_nums(self, min_pt, max_pt, nb_pixels):
+        """get_image_of_cell_nums: an int64 array (ny, nx) holding per pixel the
+        index of a cell of non-zero integral over it (the largest such index),
+        -1 where there is none."""
+        mn, mx = _f64(min_pt), _f64(max_pt)
+        nbp = np.array(nb_pixels, dtype=np.int64)
+        out = np.empty((int(nbp[1]), int(nbp[0])), dtype=np.int64)
+        self._check(self._lib.sdot_get_image_of_cell_nums(self._ctx, _ptr(mn), _ptr(mx), _ptr(nbp), _ptr(out),
+                                                          SDOT_HOST))
+        return out
 
     def solve_weights(self, target_masses, rel_mass_tol=1e-10, max_iter=150, damping=True, pcg_rel_tol=1e-12,
                       pcg_max_iter=20000, verbosity=0, preconditioner="multilevel"):

@@ -127,6 +127,33 @@ def test_image_density(gpu_lib, ref_oracle):
     assert abs(gpu.integrals().sum() - 0.8) < 1e-11
 
 
+@pytest.mark.parametrize("n,res", [(3000, (64, 64)), (100_000, (256, 200))])
+def test_image_poly6(gpu_lib, ref_oracle, n, res):
+    # piecewise-quadratic image (nb_coeffs = 6): per-pixel quadratic densities
+    rng = np.random.default_rng(610 + n)
+    p = rng.random((n, 2))
+    w = rng.uniform(-1e-2, 1e-2, n) / n
+    img = rng.uniform(-0.3, 0.3, (6,) + res)
+    img[0] += 2.0
+    gpu, ref = make_pair(p, w, ref_oracle, image=img)
+    check_all(gpu, ref, n)
+    assert abs(gpu.domain_measure() - ref.domain_measure()) <= 1e-13 * ref.domain_measure()
+
+
+def test_image_poly6_reference_kats(gpu_lib):
+    # TEST_CASE( "scaled image 1" / "scaled image 2" ), tests/test_scaled_image.cpp:56-92
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = np.array([2, 3, 4, 5, 6, 7], dtype=float).reshape(6, 1, 1)
+    g = PowerDiagram(np.array([[0.5, 0.5]]), np.array([1.0]))
+    g.set_image_density(c)
+    assert abs(g.integrals()[0] - 11) < 1e-6
+    g = PowerDiagram(np.array([[0.25, 0.25], [0.75, 0.25], [0.25, 0.75], [0.75, 0.75]]), np.ones(4))
+    g.set_image_density(c)
+    for got, exp in zip(g.integrals(), [1.28125, 2.46875, 2.84375, 4.40625]):
+        assert abs(got - exp) < 1e-6
+
+
 def test_image_density_disc_clip(gpu_lib, ref_oracle):
     c = workloads.config3(n=5000, res=128)
     gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle, radial_func="in_ball_w05", image=c["image"])
@@ -164,6 +191,35 @@ def test_convex_polyhedron_domain(gpu_lib, ref_oracle):
     nrm = np.stack([np.cos(ang), np.sin(ang)], 1)
     p = 0.5 + (rng.random((n, 2)) - 0.5) * 0.8
     shapes = [("add_convex_polyhedron_shape", (pts, nrm, 1.0))]
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, shapes=shapes)
+    check_all(gpu, ref, n)
+
+
+@pytest.mark.parametrize("sides", [20, 64])
+def test_many_sided_domain(gpu_lib, ref_oracle, sides):
+    # a domain polygon with more vertices than the fast tier's polygons:
+    # every cell starts in the warp tier
+    rng = np.random.default_rng(60 + sides)
+    n = 3000
+    ang = (np.arange(sides) + 0.5) * 2 * np.pi / sides
+    pts = np.stack([0.5 + 0.5 * np.cos(ang), 0.5 + 0.5 * np.sin(ang)], 1)
+    nrm = np.stack([np.cos(ang), np.sin(ang)], 1)
+    p = 0.5 + (rng.random((n, 2)) - 0.5) * 0.9
+    w = rng.uniform(-1e-5, 1e-5, n)
+    shapes = [("add_convex_polyhedron_shape", (pts, nrm, 1.0))]
+    gpu, ref = make_pair(p, w, ref_oracle, shapes=shapes)
+    check_all(gpu, ref, n)
+
+
+def test_many_sided_shape_among_others(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(62)
+    n = 2000
+    ang = (np.arange(24) + 0.5) * 2 * np.pi / 24
+    pts = np.stack([1.5 + 0.5 * np.cos(ang), 0.5 + 0.5 * np.sin(ang)], 1)
+    nrm = np.stack([np.cos(ang), np.sin(ang)], 1)
+    p = rng.random((n, 2)) * [2.0, 1.0]
+    shapes = [("add_box_shape", ([0.0, 0.0], [1.0, 1.0], 1.0)),
+              ("add_convex_polyhedron_shape", (pts, nrm, 0.5))]
     gpu, ref = make_pair(p, np.zeros(n), ref_oracle, shapes=shapes)
     check_all(gpu, ref, n)
 
