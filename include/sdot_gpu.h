@@ -99,6 +99,17 @@ int sdot_clear_domain(sdot_ctx *ctx);
 int sdot_normalize_domain(sdot_ctx *ctx);
 int sdot_domain_measure(sdot_ctx *ctx, double *measure);
 
+/* ---- periodicity ------------------------------------------------------------
+ * SpZGrid::translations (SpZGrid.h:53, with Pc::allow_translations): count
+ * translation vectors (x, y pairs; 2D, at most 64).  Each cell is also cut by
+ * the images x_j + t_k of every Dirac (its own images included), as the
+ * reference's traversal does (SpZGrid.tcc:558-561, :608-611); the image of
+ * Dirac j under translation k has the cut id j + (k + 1) n in the neighbour
+ * lists, and its Hessian entry goes to column j, the distance taken to the
+ * image (get_der_integrals_wrt_weights.h:61-62).  count = 0 removes them.
+ * The mixed-precision context runs its periodic cells in FP64.             */
+int sdot_set_translations(sdot_ctx *ctx, const double *translations, int64_t count);
+
 /* ---- radial function ------------------------------------------------------
  * on = 0: FunctionEnum::Unit (Unit.h:10-30); on = 1: FunctionEnum::InBallW05
  * (InBallW05.h:8-28): each cell is also clipped by the disc of radius sqrt(w_i). */

@@ -67,6 +67,7 @@ def load():
         "ref_neighbors_copy": (None, [P, P, P]),
         "ref_timings": (None, [P, P]),
         "ref_get_image_integrals": (None, [P, P, P, P, P]),
+        "ref_set_translations": (None, [P, P, I64]),
         "ref_get_image_of_cell_nums": (None, [P, P, P, P, P]),
     }
     for k, (r, a) in sig.items():
@@ -186,6 +187,11 @@ class RefPowerDiagram:
         ids = np.zeros(cnt, dtype=np.int64)
         self.L.ref_neighbors_copy(self.h, _p(off), _p(ids))
         return off, ids
+
+    def set_translations(self, translations):
+        t = _f(np.asarray(translations, dtype=np.float64).reshape(-1, self.dim))
+        self.L.ref_set_translations(self.h, _p(t), t.shape[0])
+        self._updated = False
 
     def image_integrals(self, min_pt, max_pt, nb_pixels):
         """get_image_integrals: (ny, nx, 3) per pixel (sum m x, sum m y, sum m)."""

@@ -44,7 +44,9 @@ using namespace sdot;
 
 namespace {
 
-struct Pc2 { enum { dim = 2, allow_ball_cut = 1, allow_translations = 0 }; using TI = std::size_t; using TF = double; using CI = std::size_t; };
+// allow_translations = 1 compiles the traversal's periodic branch; with no
+// translation set it takes the same path as allow_translations = 0
+struct Pc2 { enum { dim = 2, allow_ball_cut = 1, allow_translations = 1 }; using TI = std::size_t; using TF = double; using CI = std::size_t; };
 struct Pc3 { enum { dim = 3, allow_ball_cut = 0, allow_translations = 0 }; using TI = std::size_t; using TF = double; using CI = std::size_t; };
 
 // ScaledImage::for_each_intersection with the full-disc bounding box fixed.
@@ -331,6 +333,19 @@ void ref_set_image(void *h, const double *min_pt, const double *max_pt, const do
 }
 
 void ref_update(void *h) { dispatch(h, [&](auto &c) { c.update(); return 0; }); }
+// SpZGrid::translations (2D)
+void ref_set_translations(void *h, const double *t, std::int64_t count) {
+    dispatch(h, [&](auto &c) {
+        using Pt = typename std::decay_t<decltype(c)>::Pt;
+        c.grid.translations.clear();
+        for (std::int64_t k = 0; k < count; ++k) {
+            Pt p;
+            for (int d = 0; d < c.dim; ++d) p[d] = t[c.dim * k + d];
+            c.grid.translations.push_back(p);
+        }
+        return 0;
+    });
+}
 void ref_get_image_integrals(void *h, const double *lo, const double *hi, const std::int64_t *nbp, double *out) {
     dispatch(h, [&](auto &c) { c.image_integrals(lo, hi, nbp, out, false, nullptr); return 0; });
 }

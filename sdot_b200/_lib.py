@@ -89,6 +89,7 @@ SIGNATURES = {
     "sdot_normalize_domain": (ctypes.c_int, [_P]),
     "sdot_domain_measure": (ctypes.c_int, [_P, _P]),
     "sdot_set_ball_cut": (ctypes.c_int, [_P, ctypes.c_int]),
+    "sdot_set_translations": (ctypes.c_int, [_P, _P, _I64]),
     "sdot_get_integrals": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "sdot_get_centroids": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "sdot_get_der_integrals_wrt_weights": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int]),

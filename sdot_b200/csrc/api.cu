@@ -121,6 +121,11 @@ struct sdot_ctx {
     int img_ncoeffs = 1;
     std::vector<double> img_data;
     int ball = 0;
+    // periodic copies of the Diracs (SpZGrid::translations, SpZGrid.h:53): x, y pairs
+    std::vector<double> trans_h;
+    double *d_trans = nullptr;
+    // the kernel mode of a one-shape pass: with translations, the periodic walk
+    int single_mode() const { return trans_h.empty() ? DM_SINGLE : DM_PERIODIC; }
 
     // domain (device side)
     int mode = DM_SINGLE;
@@ -180,6 +185,7 @@ struct sdot_ctx {
         tree3.release();
         dfree(d_pos); dfree(d_w);
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
+        dfree(d_trans);
         free_eval();
         free_newton();
         free_multi();
@@ -274,7 +280,7 @@ struct sdot_ctx {
             coeff = 1;
         } else if (items.size() == 1) {
             // ConvexPolyhedronAssembly::englobing_convex_polyhedron with one item
-            mode = DM_SINGLE;
+            mode = single_mode();
             const Item2 &it = items[0];
             start_n = int(it.xy.size() / 2);
             dalloc(d_start, it.xy.size());
@@ -352,6 +358,8 @@ struct sdot_ctx {
         a.ovf_list = ovf_list;
         a.ovf_cnt = ovf_cnt;
         a.err = err;
+        a.ntrans = int(trans_h.size() / 2);
+        a.trans = d_trans;
         return a;
     }
 
@@ -362,8 +370,13 @@ struct sdot_ctx {
                 throw Unsupported(boxes3.empty() ? "no domain: call sdot_add_box_shape first"
                                                  : "3D domains of several boxes are not available in this build");
             if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
+            if (!trans_h.empty()) throw Unsupported("periodic translations are available in 2D only");
             return;
         }
+        if (!trans_h.empty() && (long long)(trans_h.size() / 2 + 1) * n >= (1LL << 31))
+            throw Unsupported("(translations + 1) x Diracs must stay below 2^31 (cut ids are 32-bit)");
+        if (!trans_h.empty() && has_image)
+            throw Unsupported("periodic translations with an image density are not available in this build");
         if (has_image && img_ncoeffs == 6 && ball)
             throw Unsupported("no ball cut with a piecewise-quadratic image (the reference's Polynomial<6> arc "
                               "integrals are a TODO)");
@@ -398,7 +411,7 @@ struct sdot_ctx {
         SDOT_CUDA(cudaMemsetAsync(rows.side_used, 0, sizeof(unsigned long long), stream));
         for (size_t k = 0; k + 1 < item_off_h.size(); ++k) {
             Cell2DArgs a = args();
-            a.mode = DM_SINGLE;
+            a.mode = single_mode();
             a.start_n = item_off_h[k + 1] - item_off_h[k];
             a.start_xy = d_item_xy + 2 * item_off_h[k];
             a.coeff = items[k].coeff;
@@ -579,7 +592,7 @@ struct sdot_ctx {
                 // englobing box (the cell the reference's callback receives)
                 Cell2DArgs a = args();
                 if (mode == DM_MULTI) {
-                    a.mode = DM_SINGLE;
+                    a.mode = single_mode();
                     a.coeff = 1.0;
                 }
                 a.nb = nb;
@@ -613,6 +626,7 @@ struct sdot_ctx {
         check_domain();
         if (mode == DM_IMAGE || mode == DM_IMAGE6)
             throw Unsupported("image integrals over an image density are not available in this build");
+        if (!trans_h.empty()) throw Unsupported("image integrals with periodic translations are not available");
         reserve_eval();
         ensure_tree();
         const long long np = nx * ny;
@@ -1180,6 +1194,23 @@ int sdot_domain_measure(sdot_ctx *ctx, double *measure) {
     return guarded(ctx, [&] {
         if (!measure) throw BadArg("null output");
         *measure = domain_measure(ctx);
+        return int(SDOT_OK);
+    });
+}
+
+int sdot_set_translations(sdot_ctx *ctx, const double *translations, int64_t count) {
+    return guarded(ctx, [&] {
+        if (count < 0 || (count > 0 && !translations)) throw BadArg("bad translations");
+        if (ctx->dim != 2 && count > 0) throw Unsupported("periodic translations are available in 2D only");
+        if (count > 64) throw BadArg("at most 64 translations");
+        ctx->trans_h.assign(translations, translations + 2 * count);
+        if (count) {
+            dalloc(ctx->d_trans, size_t(2 * count));
+            SDOT_CUDA(cudaMemcpy(ctx->d_trans, ctx->trans_h.data(), size_t(2 * count) * sizeof(double),
+                                 cudaMemcpyHostToDevice));
+        }
+        ctx->dom_dirty = true;
+        ctx->mark_dirty();
         return int(SDOT_OK);
     });
 }

@@ -106,6 +106,7 @@ struct Sink {
     int acc_st;
     Out &row;
     long long n_diracs = 1LL << 40;
+    const double *trans = nullptr;  // periodic domains: translation k of id j + (k + 1) n
 
     SDOT_HDI Sink(const P &c, const double *p, double x0, double y0, double sw, double r_, double *a, int ast,
                   Out &ro)
@@ -133,11 +134,24 @@ struct Sink {
         if (id < 0) return;
         const double m = coeff * len;
         if (DIRECT) {
-            const double dx = c0x - pos[2 * SDOT_CHECK_IDX(id, n_diracs, 3)], dy = c0y - pos[2 * id + 1];
+            // the neighbour, or the image of Dirac j under translation k for
+            // an id j + (k + 1) n (get_der_integrals_wrt_weights.h:61-62)
+            int j = id;
+            double qx, qy;
+            if (id >= n_diracs) {
+                const int k = int(id / n_diracs) - 1;
+                j = int(id % n_diracs);
+                qx = pos[2 * j] + trans[2 * k];
+                qy = pos[2 * j + 1] + trans[2 * k + 1];
+            } else {
+                qx = pos[2 * SDOT_CHECK_IDX(id, n_diracs, 3)];
+                qy = pos[2 * id + 1];
+            }
+            const double dx = c0x - qx, dy = c0y - qy;
             const double dist = sqrt(dx * dx + dy * dy);
             if (dist != 0) {
                 const double b = 0.5 * m / dist;
-                row.emit(id, -b);
+                row.emit(j, -b);
                 der0 += b;
             }
         } else {
@@ -356,6 +370,12 @@ SDOT_HDI void stream_cell(const P &cell, int n, Stage &st) {
 // and the handling of a needed node branch.
 // Returns the vertex count, -1 on capacity (or stack / visit cap) overflow,
 // -2 on a failed guard.
+// PER (periodic domains): after the tree, the walk visits it again once per
+// translation t, as the tree of the Diracs x_j + t (SpZGrid.tcc:558-561:
+// every translation's root enters the front; boxes and Diracs are shifted by
+// t, :396-397 and :608-611); a cut by the image of Dirac j under translation
+// k carries the id j + (k + 1) n, and the Dirac's own images cut it too.
+template <bool PER = false>
 SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double c0x, double c0y,
                         double w0) {
     int n = A.start_n;
@@ -376,9 +396,22 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
     int j = 0, je = 0;          // Diracs of the current leaf still to cut by
     double cjx = 0, cjy = 0, cjw = 0;  // Dirac j
     int visits = 0;
-    auto skip_self = [&](int k) { return k == s ? k + 1 : k; };
+    int sym = -1;               // PER: the translation of the current walk (-1: none)
+    double tx = 0, ty = 0;      // and its vector
+    auto skip_self = [&](int k) { return (!PER || sym < 0) && k == s ? k + 1 : k; };
+    // shifted by the current translation (PER only: adding a zero would not
+    // be free, it turns -0 into +0)
+    auto tr = [&](double v, double t) { return PER ? v + t : v; };
     while (true) {
         // ---- the step: one cut (j < je) or one node test
+        if (PER && j >= je && !has_top && sym + 1 < A.ntrans) {
+            // the next translation's walk starts from the root again
+            ++sym;
+            tx = A.trans[2 * sym];
+            ty = A.trans[2 * sym + 1];
+            top = 0;
+            has_top = true;
+        }
         const bool is_cut = j < je;
         double ox = 0, oy = 0, nx = 0, ny = 0;
         double lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0, maxw = 0;
@@ -390,13 +423,13 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             jn = skip_self(j + 1);
             if (jn < je) {
                 (void)SDOT_CHECK_IDX(jn, A.n, 6);
-                njx = A.pos[2 * jn];
-                njy = A.pos[2 * jn + 1];
+                njx = tr(A.pos[2 * jn], tx);
+                njy = tr(A.pos[2 * jn + 1], ty);
                 njw = A.w[jn];
             }
         } else {
             if (!has_top) break;
-            if (++visits > A.max_nodes) {  // a tree visits each node once: a cycle means a corrupt tree
+            if (++visits > (PER ? (A.ntrans + 1) * A.max_nodes : A.max_nodes)) {  // each tree walk visits a node once
                 flag_error(A.err, DE_ITER);
                 return -1;
             }
@@ -406,10 +439,10 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             else
                 has_top = false;
             const TreeNode<2> &nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
-            lo0 = nd.lo[0];
-            lo1 = nd.lo[1];
-            hi0 = nd.hi[0];
-            hi1 = nd.hi[1];
+            lo0 = tr(nd.lo[0], tx);
+            lo1 = tr(nd.lo[1], ty);
+            hi0 = tr(nd.hi[0], tx);
+            hi1 = tr(nd.hi[1], ty);
             maxw = nd.maxw;
             nd_a = nd.a;
             nd_b = nd.b;
@@ -428,7 +461,7 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
         const CutFacts f = cut_facts(mask, n);
         if (is_cut) {
             if (f.nb_out) {
-                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
+                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, PER ? j + (sym + 1) * int(A.n) : j, true, f);
                 if (n <= 0) return n;
             }
             j = jn;
@@ -452,8 +485,8 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             int ch[4];
             for (int c = 0; c < nch; ++c) {
                 const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
-                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
-                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
+                const double mx = c0x - tr(0.5 * (cn.lo[0] + cn.hi[0]), tx);
+                const double my = c0y - tr(0.5 * (cn.lo[1] + cn.hi[1]), ty);
                 key[c] = float(mx * mx + my * my);
                 ch[c] = first + c;
             }
@@ -482,8 +515,8 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             j = skip_self(nd_a);
             je = nd_b;
             if (j < je) {
-                cjx = A.pos[2 * j];
-                cjy = A.pos[2 * j + 1];
+                cjx = tr(A.pos[2 * j], tx);
+                cjy = tr(A.pos[2 * j + 1], ty);
                 cjw = A.w[j];
             }
         }
@@ -789,12 +822,13 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
         raster_cell<BALL>(A, s, cell, n, c0x, c0y, r);
         return true;
     }
-    constexpr bool DIRECT = MODE == DM_SINGLE;
+    constexpr bool DIRECT = MODE == DM_SINGLE || MODE == DM_PERIODIC;
     using SinkT = Sink<DIRECT, P, MODE == DM_IMAGE6>;
     SinkT sink(cell, A.pos, c0x, c0y, BALL ? r : sqrt(w0), r, acc, acc_st, row);
     sink.n_diracs = A.n;
+    sink.trans = A.trans;
 
-    if (MODE == DM_SINGLE && !BALL) {
+    if (DIRECT && !BALL) {
         // reference order: fan from vertex 0, boundary items from edge (n-1 -> 0)
         double tr2 = 0;
         for (int i = 2; i < n; ++i) {
@@ -814,7 +848,7 @@ SDOT_KFN bool finish_cell(const Cell2DArgs &A, long long s, const P &cell, int n
             const double dx = cell.X(i1) - cell.X(i0), dy = cell.Y(i1) - cell.Y(i0);
             sink.line(i0, sqrt(dx * dx + dy * dy));
         }
-    } else if (MODE == DM_SINGLE) {
+    } else if (DIRECT) {
         sink.begin_piece(A.coeff);
         DiscClip<SinkT> dc(sink, c0x, c0y, r);
         stream_cell(cell, n, dc);
@@ -944,7 +978,7 @@ __global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d(const Cell2DArgs A) {
     double *acc = extra + t;
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
-    const int n = build_cell(A, s, cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s]);
+    const int n = build_cell<MODE == DM_PERIODIC>(A, s, cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s]);
     Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
     Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
     if (finish_cell<MODE, BALL>(A, s, cell, n, acc, T2D, row, nbo)) {
@@ -1042,6 +1076,7 @@ __device__ bool commit(const Rows &R, long long s, const int *col, const double 
 // Warp-per-cell build of one large cell (all lanes, same s): the walk of
 // build_cell, with the eviction test and the plane cuts spread over the
 // lanes, 32 vertices at a time.
+template <bool PER = false>
 __device__ int build_cell_coop(const Cell2DArgs &A, long long s, const PolyView<double> &cell, int cap, double c0x,
                                double c0y, double w0, int *wstack) {
     constexpr unsigned FULL = 0xffffffffu;
@@ -1053,83 +1088,95 @@ __device__ int build_cell_coop(const Cell2DArgs &A, long long s, const PolyView<
             cell.Y(k) = A.start_xy[2 * k + 1];
             cell.I(k) = domain_id(k);
         }
-        wstack[0] = 0;
     }
     __syncwarp();
-    int sp = 1;
-    for (int visits = 0; sp > 0; ++visits) {
-        if (visits > A.max_nodes) {
-            if (lane == 0) flag_error(A.err, DE_ITER);
-            return -1;
-        }
-        const int node = wstack[--sp];
+    int visits = 0;
+    // PER: one walk of the tree per translation after the untranslated one
+    // (see build_cell)
+    for (int sym = -1; sym < (PER ? A.ntrans : 0); ++sym) {
+        const double tx = sym >= 0 ? A.trans[2 * sym] : 0.0, ty = sym >= 0 ? A.trans[2 * sym + 1] : 0.0;
+        if (lane == 0) wstack[0] = 0;
         __syncwarp();
-        const TreeNode<2> nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
-        bool need = false;
-        for (int base = 0; base < n; base += 32) {
-            const int k = base + lane;
-            bool fail = false;
-            if (k < n) {
-                const double px = cell.X(k), py = cell.Y(k);
-                const double qx = fmin(nd.hi[0], fmax(nd.lo[0], px));
-                const double qy = fmin(nd.hi[1], fmax(nd.lo[1], py));
-                const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
-                const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - nd.maxw;
-                fail = !(lhs <= rhs);
-            }
-            if (__any_sync(FULL, fail)) {
-                need = true;
-                break;
-            }
-        }
-        if (!need) continue;
-        if (nd.b < 0) {
-            const int first = nd.a, nch = -nd.b;
-            if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
-                if (lane == 0) guard_fail(A, 1, s, node);
-                return -2;
-            }
-            if (sp + nch > STACK) {
-                if (lane == 0) flag_error(A.err, DE_STACK);
+        int sp = 1;
+        for (; sp > 0; ++visits) {
+            if (visits > (PER ? (A.ntrans + 1) * A.max_nodes : A.max_nodes)) {
+                if (lane == 0) flag_error(A.err, DE_ITER);
                 return -1;
             }
-            float key[4];
-            int ch[4];
-            for (int c = 0; c < nch; ++c) {
-                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
-                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
-                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
-                key[c] = float(mx * mx + my * my);
-                ch[c] = first + c;
-            }
-            for (int i = 1; i < nch; ++i) {  // farthest first
-                const float kk = key[i];
-                const int cc = ch[i];
-                int j = i - 1;
-                while (j >= 0 && key[j] < kk) {
-                    key[j + 1] = key[j];
-                    ch[j + 1] = ch[j];
-                    --j;
-                }
-                key[j + 1] = kk;
-                ch[j + 1] = cc;
-            }
-            if (lane == 0)
-                for (int c = 0; c < nch; ++c) wstack[sp + c] = ch[c];
+            const int node = wstack[--sp];
             __syncwarp();
-            sp += nch;
-        } else {
-            if (nd.a < 0 || nd.b > A.n) {
-                if (lane == 0) guard_fail(A, 2, s, node);
-                return -2;
+            const TreeNode<2> nd = A.nodes[SDOT_CHECK_IDX(node, A.max_nodes, 4)];
+            const double lo0 = PER ? nd.lo[0] + tx : nd.lo[0], lo1 = PER ? nd.lo[1] + ty : nd.lo[1];
+            const double hi0 = PER ? nd.hi[0] + tx : nd.hi[0], hi1 = PER ? nd.hi[1] + ty : nd.hi[1];
+            bool need = false;
+            for (int base = 0; base < n; base += 32) {
+                const int k = base + lane;
+                bool fail = false;
+                if (k < n) {
+                    const double px = cell.X(k), py = cell.Y(k);
+                    const double qx = fmin(hi0, fmax(lo0, px));
+                    const double qy = fmin(hi1, fmax(lo1, py));
+                    const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
+                    const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - nd.maxw;
+                    fail = !(lhs <= rhs);
+                }
+                if (__any_sync(FULL, fail)) {
+                    need = true;
+                    break;
+                }
             }
-            for (int j = nd.a; j < nd.b; ++j) {
-                if (j == s) continue;
-                const double c1x = A.pos[2 * j], c1y = A.pos[2 * j + 1], w1 = A.w[j];
-                double ox, oy, nx, ny;
-                bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
-                n = plane_cut_warp(cell, n, cap, ox, oy, nx, ny, j, true);
-                if (n <= 0) return n;
+            if (!need) continue;
+            if (nd.b < 0) {
+                const int first = nd.a, nch = -nd.b;
+                if (nch < 2 || nch > 4 || first < 1 || first + nch > A.max_nodes) {
+                    if (lane == 0) guard_fail(A, 1, s, node);
+                    return -2;
+                }
+                if (sp + nch > STACK) {
+                    if (lane == 0) flag_error(A.err, DE_STACK);
+                    return -1;
+                }
+                float key[4];
+                int ch[4];
+                for (int c = 0; c < nch; ++c) {
+                    const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
+                    const double cx = 0.5 * (cn.lo[0] + cn.hi[0]), cy = 0.5 * (cn.lo[1] + cn.hi[1]);
+                    const double mx = c0x - (PER ? cx + tx : cx);
+                    const double my = c0y - (PER ? cy + ty : cy);
+                    key[c] = float(mx * mx + my * my);
+                    ch[c] = first + c;
+                }
+                for (int i = 1; i < nch; ++i) {  // farthest first
+                    const float kk = key[i];
+                    const int cc = ch[i];
+                    int j = i - 1;
+                    while (j >= 0 && key[j] < kk) {
+                        key[j + 1] = key[j];
+                        ch[j + 1] = ch[j];
+                        --j;
+                    }
+                    key[j + 1] = kk;
+                    ch[j + 1] = cc;
+                }
+                if (lane == 0)
+                    for (int c = 0; c < nch; ++c) wstack[sp + c] = ch[c];
+                __syncwarp();
+                sp += nch;
+            } else {
+                if (nd.a < 0 || nd.b > A.n) {
+                    if (lane == 0) guard_fail(A, 2, s, node);
+                    return -2;
+                }
+                for (int j = nd.a; j < nd.b; ++j) {
+                    if (j == s && sym < 0) continue;
+                    const double c1x = PER ? A.pos[2 * j] + tx : A.pos[2 * j];
+                    const double c1y = PER ? A.pos[2 * j + 1] + ty : A.pos[2 * j + 1];
+                    const double w1 = A.w[j];
+                    double ox, oy, nx, ny;
+                    bisector(c0x, c0y, w0, c1x, c1y, w1, ox, oy, nx, ny);
+                    n = plane_cut_warp(cell, n, cap, ox, oy, nx, ny, PER ? j + (sym + 1) * int(A.n) : j, true);
+                    if (n <= 0) return n;
+                }
             }
         }
     }
@@ -1150,7 +1197,8 @@ __global__ void __launch_bounds__(128) k_cells2d_wtier(const Cell2DArgs A, doubl
     const int cnt = *list_cnt;
     for (int i = gw; i < cnt; i += nwarps) {
         const long long s = list[i];
-        const int n = build_cell_coop(A, s, W.cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s], wstack[wb]);
+        const int n = build_cell_coop<MODE == DM_PERIODIC>(A, s, W.cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s],
+                                                           wstack[wb]);
         if (lane == 0) {
             Out row(A.rows.cnt ? W.row_col : nullptr, W.row_val, 1, CAP + 1);
             Out nbo(A.nb.cnt ? W.nb_id : nullptr, nullptr, 1, 2 * CAP);
@@ -1284,6 +1332,11 @@ void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
     const bool ball = a.ball != 0;
     if (a.mode == DM_SINGLE) {
         if (ball) launch_all<DM_SINGLE, true>(a, scratch, st); else launch_all<DM_SINGLE, false>(a, scratch, st);
+    } else if (a.mode == DM_PERIODIC) {
+        // the mixed path has no periodic walk: the FP64 kernels run
+        Cell2DArgs b = a;
+        b.mixed = 0;
+        if (ball) launch_all<DM_PERIODIC, true>(b, scratch, st); else launch_all<DM_PERIODIC, false>(b, scratch, st);
     } else if (a.mode == DM_IMAGE) {
         if (ball) launch_all<DM_IMAGE, true>(a, scratch, st); else launch_all<DM_IMAGE, false>(a, scratch, st);
     } else if (a.mode == DM_RASTER) {

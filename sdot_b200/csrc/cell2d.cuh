@@ -10,7 +10,8 @@ namespace sdot {
 // DM_RASTER: no cell outputs; each cell (with the starting shape's density)
 // is integrated over the pixels of a raster (get_image_integrals,
 // get_image_of_cell_nums)
-enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2, DM_IMAGE6 = 3, DM_RASTER = 4 };
+// DM_PERIODIC: DM_SINGLE with translated copies of the Diracs (ntrans > 0)
+enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2, DM_IMAGE6 = 3, DM_RASTER = 4, DM_PERIODIC = 5 };
 
 // Cell polygon capacities of the two tiers.  Every cell is first built by
 // the fast kernel (one thread per cell, polygon in shared memory); cells that
@@ -91,6 +92,10 @@ struct Cell2DArgs {
     double ras_lo[2] = {0, 0}, ras_hi[2] = {1, 1};
     int ras_nx = 0, ras_ny = 0;
     const int *perm = nullptr;     // sorted -> caller index
+    // periodic domains (DM_PERIODIC): ntrans translations (x, y pairs); the
+    // image of sorted Dirac j under translation k cuts with id j + (k + 1) n
+    int ntrans = 0;
+    const double *trans = nullptr;
     unsigned *err = nullptr;
     int *guard = nullptr;          // first failed guard: (code, sorted index, value)
     long long item_nv = 0;         // number of item vertices (multi items)

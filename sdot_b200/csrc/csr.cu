@@ -96,7 +96,8 @@ __global__ void k_nb_write(Rows NB, long long n, const int *idx, const long long
     const long long o = offsets[idx[s]];
     for (int i = 0; i < m; ++i) {
         const int id = *NB.colp(s, i);
-        ids[o + i] = id >= 0 ? (long long)idx[id] : (id == ID_ARC ? -2 : -1);
+        // periodic images: id j + (k + 1) n keeps its translation k
+        ids[o + i] = id >= 0 ? (long long)idx[id % n] + (long long)(id / n) * n : (id == ID_ARC ? -2 : -1);
     }
 }
 

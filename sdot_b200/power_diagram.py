@@ -143,6 +143,13 @@ class PowerDiagram:
         self._check(self._lib.sdot_domain_measure(self._ctx, _ptr(out)))
         return float(out[0])
 
+    def set_translations(self, translations):
+        """Periodic copies of the Diracs (SpZGrid::translations): a list of
+        translation vectors; each cell is also cut by the images of every
+        Dirac under them.  An empty list removes them."""
+        t = _f64(np.asarray(translations, dtype=np.float64).reshape(-1, self.dim))
+        self._check(self._lib.sdot_set_translations(self._ctx, _ptr(t) if t.size else None, int(t.shape[0])))
+
     def set_radial_func(self, name):
         on = {"unit": 0, "in_ball_w05": 1}[name]
         self.radial_func = name

@@ -237,3 +237,43 @@ def test_deterministic_repeat(gpu_lib):
     assert np.array_equal(outs[0][0], outs[1][0])
     for a, b in zip(outs[0][1], outs[1][1]):
         assert np.array_equal(a, b)
+
+
+# ---- periodic domains (SpZGrid::translations): the unit cell repeated by the
+# 8 translations around it, domain [-1, 2]^2 as the reference's periodic
+# benchmark sets it up (benchmarks/bench_volume_2D.cpp:54-64)
+PERIODIC_T = [(x, y) for x in (-1.0, 0.0, 1.0) for y in (-1.0, 0.0, 1.0) if x or y]
+
+
+def periodic_pair(p, w, ref_oracle, radial_func="unit"):
+    shapes = [("add_box_shape", ([-1.0, -1.0], [2.0, 2.0], 1.0))]
+    gpu, ref = make_pair(p, w, ref_oracle, radial_func=radial_func, shapes=shapes)
+    gpu.set_translations(PERIODIC_T)
+    ref.set_translations(PERIODIC_T)
+    return gpu, ref
+
+
+@pytest.mark.parametrize("n", [50, 3000])
+def test_periodic_uniform(gpu_lib, ref_oracle, n):
+    rng = np.random.default_rng(80 + n)
+    p = rng.random((n, 2))
+    w = rng.uniform(-1e-6, 1e-6, n)
+    gpu, ref = periodic_pair(p, w, ref_oracle)
+    check_all(gpu, ref, n)
+    assert abs(gpu.integrals().sum() - 1.0) < 1e-12  # the cells tile the torus
+
+
+def test_periodic_clustered(gpu_lib, ref_oracle):
+    c = workloads.config2(n=50_000)
+    p = c["positions"]
+    gpu, ref = periodic_pair(p, c["weights"], ref_oracle)
+    check_all(gpu, ref, len(p), rtol_hess=1e-10)
+
+
+def test_periodic_disc_clip(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(83)
+    n = 2000
+    p = rng.random((n, 2))
+    w = np.full(n, 0.3 / n) * rng.uniform(0.5, 2.0, n)
+    gpu, ref = periodic_pair(p, w, ref_oracle, radial_func="in_ball_w05")
+    check_all(gpu, ref, n, rtol=1e-11)
