@@ -189,6 +189,10 @@ typedef struct sdot_newton_opts {
     int damping;           /* 0: reference rule, 1: KMT step halving */
     int verbosity;         /* > 0: one line per Newton iteration on stderr */
     int preconditioner;    /* 0: multilevel (default), 1: Jacobi */
+    int pcg_fp32;          /* 1: each linear solve by FP32 PCG on an FP32 copy of the Hessian
+                              with FP64 iterative refinement (FP64 residuals, FP64 weights;
+                              steps that do not halve the residual hand over to FP64 PCG);
+                              0: FP64 PCG */
 } sdot_newton_opts;
 
 typedef struct sdot_newton_report {
@@ -202,7 +206,7 @@ typedef struct sdot_newton_report {
 } sdot_newton_report;
 
 /* target: double[n] masses (mem_space says where).  opts may be NULL for the
- * defaults {150, 1e-10, 20000, 1e-12, 1, 0, 0}; report may be NULL.
+ * defaults {150, 1e-10, 20000, 1e-12, 1, 0, 0, 0}; report may be NULL.
  * Returns SDOT_OK, SDOT_NOT_CONVERGED (iteration or step-halving cap),
  * SDOT_VOID_CELL (damping = 1 and a cell is empty at the start weights) or
  * an evaluation error.                                                        */

@@ -43,6 +43,7 @@ class SdotNewtonOptions(ctypes.Structure):
         ("damping", ctypes.c_int),
         ("verbosity", ctypes.c_int),
         ("preconditioner", ctypes.c_int),
+        ("pcg_fp32", ctypes.c_int),
     ]
 
 

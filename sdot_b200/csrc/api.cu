@@ -693,10 +693,36 @@ struct sdot_ctx {
     double *t_orig = nullptr, *t_sorted = nullptr, *w_old = nullptr, *dir = nullptr, *rhs = nullptr;
     double *pcg_buf = nullptr, *red = nullptr, *mg_buf = nullptr;
     PcgWork pcg;
+    // FP32 solves with FP64 refinement: FP32 copies of the Hessian values,
+    // FP32 work vectors and multilevel storage, the refinement's residual
+    double *pcg32_buf = nullptr, *mg32_buf = nullptr, *ref_buf = nullptr;
+    float *val32 = nullptr, *side32 = nullptr;
+    long long side32_cap = 0, f32cap = 0;
+    PcgWorkT<float> pcg32;
 
     void free_newton() {
         dfree(t_orig); dfree(t_sorted); dfree(w_old); dfree(dir); dfree(rhs); dfree(pcg_buf); dfree(red); dfree(mg_buf);
+        dfree(pcg32_buf); dfree(mg32_buf); dfree(ref_buf); dfree(val32); dfree(side32);
+        side32_cap = f32cap = 0;
         ncap = 0;
+    }
+    void reserve_fp32() {
+        if (f32cap < n || !val32) {
+            const long long c = std::max<long long>(n, 1);
+            dalloc(pcg32_buf, pcg_work_doubles(c));
+            dalloc(mg32_buf, mg_work_doubles(c, dim == 3 ? 128 : 64));
+            dalloc(ref_buf, size_t(2 * c));
+            dalloc(val32, size_t(rows.cap) * size_t(rows.stride));
+            pcg_bind(pcg32, pcg32_buf, c);
+            pcg32.mg = mg32_buf;
+            pcg32.mg_cap = dim == 3 ? 128 : 64;
+            pcg32.mg_doubles = mg_work_doubles(c, pcg32.mg_cap);
+            f32cap = c;
+        }
+        if (side32_cap < rows.side_cap || !side32) {
+            dalloc(side32, size_t(rows.side_cap));
+            side32_cap = rows.side_cap;
+        }
     }
     void reserve_newton() {
         if (ncap >= n && t_orig) return;
@@ -780,8 +806,16 @@ struct sdot_ctx {
             }
             SDOT_CUDA(cudaMemcpyAsync(w_old, d_w, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, stream));
             axpby(s_mass, t_sorted, rhs, 1.0, -1.0, n, stream);  // v_values -= masses (.tcc:89-90)
-            const PcgResult pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream, 32,
-                                           stream != nullptr, o.preconditioner == 0);
+            PcgResult pr;
+            if (o.pcg_fp32) {
+                reserve_fp32();
+                rows_to_float(rows, n, val32, side32, stream);
+                pr = pcg_solve_refined(rows, val32, side32, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg,
+                                       pcg32, ref_buf, stream, 1e-4, 32, o.preconditioner == 0);
+            } else {
+                pr = pcg_solve(rows, n, gauge, rhs, dir, o.pcg_rel_tol, o.pcg_max_iter, pcg, stream, 32,
+                               stream != nullptr, o.preconditioner == 0);
+            }
             rep.pcg_iterations += pr.iterations;
             rep.pcg_levels = pr.levels;
             if (o.verbosity > 0)
@@ -1340,7 +1374,7 @@ int sdot_get_image_of_cell_nums(sdot_ctx *ctx, const double *min_pt, const doubl
 int sdot_solve(sdot_ctx *ctx, const double *target, int mem_space, const sdot_newton_opts *opts,
                sdot_newton_report *report) {
     return guarded(ctx, [&] {
-        sdot_newton_opts o{150, 1e-10, 20000, 1e-12, 1, 0, 0};
+        sdot_newton_opts o{150, 1e-10, 20000, 1e-12, 1, 0, 0, 0};
         if (opts) o = *opts;
         sdot_newton_report r{};
         ctx->last_error.clear();

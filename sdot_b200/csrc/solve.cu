@@ -6,6 +6,7 @@
 // only reads |r|^2 every `check` iterations to decide to stop.
 #include "solve.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 namespace sdot {
@@ -29,48 +30,61 @@ __device__ double block_sum(double v, double *sh) {
     return r;  // valid in thread 0
 }
 
-// Matrix views for the PCG kernels: row s times x, and the diagonal entry.
-struct RowsMat {
+// Matrix views for the PCG kernels: row s times x, and the diagonal entry
+// (sums in double whatever the precision of the values and vectors).
+// RowsMatT: the Hessian rows (ELL + side buffer) with values of type V
+// (rows.val itself, or an FP32 copy in the same layout).
+template <class V>
+struct RowsMatT {
     Rows R;
-    __device__ double row_dot(long long s, const double *x) const {
+    const V *val;
+    const V *side_val;
+    template <class X>
+    __device__ double row_dot(long long s, const X *x) const {
         const int m = R.cnt[s];
         double acc = 0;
         if (m <= R.cap) {
-            for (int k = 0; k < m; ++k) acc += R.val[k * R.stride + s] * x[R.col[k * R.stride + s]];
+            for (int k = 0; k < m; ++k) acc += double(val[k * R.stride + s]) * double(x[R.col[k * R.stride + s]]);
         } else {
             const long long o = R.side[s];
-            for (int k = 0; k < m; ++k) acc += R.side_val[o + k] * x[R.side_col[o + k]];
+            for (int k = 0; k < m; ++k) acc += double(side_val[o + k]) * double(x[R.side_col[o + k]]);
         }
         return acc;
+    }
+    __device__ int len(long long s) const { return R.cnt[s]; }
+    __device__ long long colk(long long s, int k) const { return *R.colp(s, k); }
+    __device__ double valk(long long s, int k) const {
+        return R.cnt[s] > R.cap ? double(side_val[R.side[s] + k]) : double(val[k * R.stride + s]);
     }
     __device__ double diag(long long s) const {
         double d = 0;
         for (int k = 0, m = R.cnt[s]; k < m; ++k)
-            if (*R.colp(s, k) == s) d += *R.valp(s, k);
+            if (colk(s, k) == s) d += valk(s, k);
         return d;
     }
-    __device__ int len(long long s) const { return R.cnt[s]; }
-    __device__ long long colk(long long s, int k) const { return *R.colp(s, k); }
-    __device__ double valk(long long s, int k) const { return *R.valp(s, k); }
     // sum_k a_sk f(col_sk)
     template <class F>
     __device__ double row_sum(long long s, const F &f) const {
         const int m = R.cnt[s];
         double acc = 0;
         if (m <= R.cap) {
-            for (int k = 0; k < m; ++k) acc += R.val[k * R.stride + s] * f(R.col[k * R.stride + s]);
+            for (int k = 0; k < m; ++k) acc += double(val[k * R.stride + s]) * f(R.col[k * R.stride + s]);
         } else {
             const long long o = R.side[s];
-            for (int k = 0; k < m; ++k) acc += R.side_val[o + k] * f(R.side_col[o + k]);
+            for (int k = 0; k < m; ++k) acc += double(side_val[o + k]) * f(R.side_col[o + k]);
         }
         return acc;
     }
 };
+using RowsMat = RowsMatT<double>;
+inline RowsMat rows_mat(const Rows &R) { return RowsMat{R, R.val, R.side_val}; }
+
 struct CsrView {
     CsrMat M;
-    __device__ double row_dot(long long s, const double *x) const {
+    template <class X>
+    __device__ double row_dot(long long s, const X *x) const {
         double acc = 0;
-        for (long long k = M.off[s], e = M.off[s + 1]; k < e; ++k) acc += M.val[k] * x[M.col[k]];
+        for (long long k = M.off[s], e = M.off[s + 1]; k < e; ++k) acc += M.val[k] * double(x[M.col[k]]);
         return acc;
     }
     __device__ double diag(long long s) const {
@@ -103,47 +117,48 @@ constexpr int MG_CAP_MAX = 128;  // coarse ELL width: w.mg_cap (64 in 2D, 128 in
 constexpr int MG_COARSE = 48;  // dense coarsest level: two 48 x 49 doubles in shared memory
 constexpr double MG_OMEGA = 0.67;
 
-struct EllView {
+template <class V>
+struct EllViewT {
     const int *cnt;
     const int *col;
-    const double *val;
+    const V *val;
     long long stride;
     __device__ int len(long long s) const { return cnt[s]; }
     __device__ long long colk(long long s, int k) const { return col[k * stride + s]; }
-    __device__ double valk(long long s, int k) const { return val[k * stride + s]; }
+    __device__ double valk(long long s, int k) const { return double(val[k * stride + s]); }
     template <class F>
     __device__ double row_sum(long long s, const F &f) const {
         double acc = 0;
-        for (int k = 0, m = cnt[s]; k < m; ++k) acc += val[k * stride + s] * f(col[k * stride + s]);
+        for (int k = 0, m = cnt[s]; k < m; ++k) acc += double(val[k * stride + s]) * f(col[k * stride + s]);
         return acc;
     }
 };
 
-template <class M>
-__global__ void k_diag_inv(M A, long long n, long long g, double *dinv, double *scal) {
+template <class M, class T>
+__global__ void k_diag_inv(M A, long long n, long long g, T *dinv, double *scal) {
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
         double d = A.diag(s);
         if (s == g) {
             scal[S_GDIAG] = d;
             d *= 2;
         }
-        dinv[s] = d != 0 ? 1.0 / d : 0.0;
+        dinv[s] = T(d != 0 ? 1.0 / d : 0.0);
     }
 }
 
-__global__ void k_init(const double *b, double *x, double *r, double *z, double *p, const double *dinv, double *partial,
-                       long long n) {
+template <class T>
+__global__ void k_init(const T *b, T *x, T *r, T *z, T *p, const T *dinv, double *partial, long long n) {
     __shared__ double sh[32];
     double rz = 0, rr = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-        const double rv = b[s];
-        const double zv = dinv[s] * rv;
+        const T rv = b[s];
+        const T zv = dinv[s] * rv;
         x[s] = 0;
         r[s] = rv;
         z[s] = zv;
         p[s] = zv;
-        rz += rv * zv;
-        rr += rv * rv;
+        rz += double(rv) * double(zv);
+        rr += double(rv) * double(rv);
     }
     rz = block_sum(rz, sh);
     rr = block_sum(rr, sh);
@@ -183,16 +198,16 @@ __global__ void k_final(const double *partial, int nb, double *scal, int mode) {
     }
 }
 
-template <class M>
-__global__ void k_spmv(M A, long long n, long long g, const double *p, double *q, const double *scal,
-                       double *partial) {
+template <class M, class T>
+__global__ void k_spmv(M A, long long n, long long g, const T *p, T *q, const double *scal, double *partial) {
     __shared__ double sh[32];
     double pq = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
         double v = A.row_dot(s, p);
-        if (s == g) v += scal[S_GDIAG] * p[s];
-        q[s] = v;
-        pq += p[s] * v;
+        if (s == g) v += scal[S_GDIAG] * double(p[s]);
+        const T qv = T(v);
+        q[s] = qv;
+        pq += double(p[s]) * double(qv);
     }
     pq = block_sum(pq, sh);
     if (threadIdx.x == 0) {
@@ -201,19 +216,20 @@ __global__ void k_spmv(M A, long long n, long long g, const double *p, double *q
     }
 }
 
-__global__ void k_update(double *x, double *r, double *z, const double *p, const double *q, const double *dinv,
-                         const double *scal, double *partial, long long n) {
+template <class T>
+__global__ void k_update(T *x, T *r, T *z, const T *p, const T *q, const T *dinv, const double *scal, double *partial,
+                         long long n) {
     __shared__ double sh[32];
-    const double alpha = scal[S_ALPHA];
+    const T alpha = T(scal[S_ALPHA]);
     double rz = 0, rr = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
         x[s] += alpha * p[s];
-        const double rv = r[s] - alpha * q[s];
+        const T rv = r[s] - alpha * q[s];
         r[s] = rv;
-        const double zv = dinv[s] * rv;
+        const T zv = dinv[s] * rv;
         z[s] = zv;
-        rz += rv * zv;
-        rr += rv * rv;
+        rz += double(rv) * double(zv);
+        rr += double(rv) * double(rv);
     }
     rz = block_sum(rz, sh);
     rr = block_sum(rr, sh);
@@ -223,8 +239,9 @@ __global__ void k_update(double *x, double *r, double *z, const double *p, const
     }
 }
 
-__global__ void k_pupdate(const double *z, double *p, const double *scal, long long n) {
-    const double beta = scal[S_BETA];
+template <class T>
+__global__ void k_pupdate(const T *z, T *p, const double *scal, long long n) {
+    const T beta = T(scal[S_BETA]);
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
         p[s] = z[s] + beta * p[s];
 }
@@ -296,8 +313,8 @@ __global__ void k_gather_sorted(const double *t, const int *idx, double *out, lo
 // 32 SLOTS entries (SLOTS per lane), so the sums have a fixed order.  The
 // gauge term of the fine level joins the coarse diagonal.  A row with more
 // than 32 SLOTS coarse columns sets *flag (the solve falls back to Jacobi).
-template <class M, int SLOTS>
-__global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *scal, MgLevel out, int *flag) {
+template <class M, int SLOTS, class T>
+__global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *scal, MgLevelT<T> out, int *flag) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -348,13 +365,13 @@ __global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *s
         for (int q = 0; q < SLOTS; ++q)
             if (lane + 32 * q < count) {
                 out.col[(lane + 32 * q) * out.n + c] = key[q];
-                out.val[(lane + 32 * q) * out.n + c] = v[q];
+                out.val[(lane + 32 * q) * out.n + c] = T(v[q]);
                 if (key[q] == c) diag = v[q];
             }
         for (int o = 16; o > 0; o >>= 1) diag += __shfl_xor_sync(FULL, diag, o);
         if (lane == 0) {
             out.cnt[c] = count;
-            out.dinv[c] = diag > 0 ? 1.0 / diag : 0.0;
+            out.dinv[c] = T(diag > 0 ? 1.0 / diag : 0.0);
             if (over) atomicExch(flag, 1);
         }
     }
@@ -363,43 +380,43 @@ __global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *s
 // Pre-smoothing and restriction of one level: z = w D^-1 r, and
 // rc[aggregate] = sum over its rows of (r - A z).  Rows are taken a block at a
 // time so that the MG_B rows of an aggregate sit in consecutive lanes.
-template <class M>
-__global__ void k_mg_pre(M A, long long n, long long gauge, const double *scal, const double *dinv, const double *r,
-                         double *z, double *rc) {
+template <class M, class T>
+__global__ void k_mg_pre(M A, long long n, long long gauge, const double *scal, const T *dinv, const T *r, T *z,
+                         T *rc) {
     const unsigned FULL = 0xffffffffu;
     for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
         const long long i = i0 + threadIdx.x;
         double t = 0;
         if (i < n) {
-            const double ri = r[i];
-            const double zi = MG_OMEGA * dinv[i] * ri;
-            z[i] = zi;
-            double acc = A.row_sum(i, [&](long long j) { return MG_OMEGA * dinv[j] * r[j]; });
+            const double ri = double(r[i]);
+            const double zi = MG_OMEGA * double(dinv[i]) * ri;
+            z[i] = T(zi);
+            double acc = A.row_sum(i, [&](long long j) { return MG_OMEGA * double(dinv[j]) * double(r[j]); });
             if (i == gauge) acc += scal[S_GDIAG] * zi;
             t = ri - acc;
         }
         for (int o = MG_B / 2; o > 0; o >>= 1) t += __shfl_down_sync(FULL, t, o, MG_B);
-        if ((threadIdx.x & (MG_B - 1)) == 0 && i < n) rc[i / MG_B] = t;
+        if ((threadIdx.x & (MG_B - 1)) == 0 && i < n) rc[i / MG_B] = T(t);
     }
 }
 
 // Coarse correction and post-smoothing: z' = z + P zc, zo = z' + w D^-1 (r - A z').
 // On the finest level (FINE) it also sums r . zo per block into partial[]
 // and, when p is given, writes p = zo (the first CG direction).
-template <class M, bool FINE>
-__global__ void k_mg_post(M A, long long n, long long gauge, const double *scal, const double *dinv, const double *r,
-                          const double *z, const double *zc, double *zo, double *partial, double *p) {
+template <class M, bool FINE, class T>
+__global__ void k_mg_post(M A, long long n, long long gauge, const double *scal, const T *dinv, const T *r, const T *z,
+                          const T *zc, T *zo, double *partial, T *p) {
     __shared__ double sh[32];
     double rz = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        auto zp = [&](long long j) { return z[j] + zc[j / MG_B]; };
+        auto zp = [&](long long j) { return double(z[j]) + double(zc[j / MG_B]); };
         const double zi = zp(i);
         double acc = A.row_sum(i, zp);
         if (i == gauge) acc += scal[S_GDIAG] * zi;
-        const double v = zi + MG_OMEGA * dinv[i] * (r[i] - acc);
+        const T v = T(zi + MG_OMEGA * double(dinv[i]) * (double(r[i]) - acc));
         zo[i] = v;
         if (FINE) {
-            rz += r[i] * v;
+            rz += double(r[i]) * double(v);
             if (p) p[i] = v;
         }
     }
@@ -413,7 +430,8 @@ __global__ void k_mg_post(M A, long long n, long long gauge, const double *scal,
 // MG_COARSE threads, thread t owns row t).  Gauss-Jordan without pivoting
 // (the matrix is symmetric positive semi-definite); a pivot below 1e-13 of
 // the largest diagonal entry marks a null direction, left out of the inverse.
-__global__ void k_mg_coarsest_setup(EllView A, int nc, double *cinv) {
+template <class V>
+__global__ void k_mg_coarsest_setup(EllViewT<V> A, int nc, double *cinv) {
     __shared__ double M[MG_COARSE][MG_COARSE + 1], I[MG_COARSE][MG_COARSE + 1];
     __shared__ double dmax;
     const int t = threadIdx.x;
@@ -422,7 +440,7 @@ __global__ void k_mg_coarsest_setup(EllView A, int nc, double *cinv) {
             M[t][c] = 0;
             I[t][c] = c == t ? 1.0 : 0.0;
         }
-        for (int k = 0, m = A.cnt[t]; k < m; ++k) M[t][A.col[k * A.stride + t]] += A.val[k * A.stride + t];
+        for (int k = 0, m = A.cnt[t]; k < m; ++k) M[t][A.col[k * A.stride + t]] += double(A.val[k * A.stride + t]);
     }
     __syncthreads();
     if (t == 0) {
@@ -456,40 +474,42 @@ __global__ void k_mg_coarsest_setup(EllView A, int nc, double *cinv) {
         for (int c = 0; c < nc; ++c) cinv[t * nc + c] = I[t][c];
 }
 
-__global__ void k_mg_coarsest_apply(const double *cinv, int nc, const double *r, double *zo) {
+template <class T>
+__global__ void k_mg_coarsest_apply(const double *cinv, int nc, const T *r, T *zo) {
     const int t = threadIdx.x;
     if (t < nc) {
         double acc = 0;
-        for (int c = 0; c < nc; ++c) acc += cinv[t * nc + c] * r[c];
-        zo[t] = acc;
+        for (int c = 0; c < nc; ++c) acc += cinv[t * nc + c] * double(r[c]);
+        zo[t] = T(acc);
     }
 }
 
 // CG start and update for the multilevel preconditioner: z, p and r . z come
 // from the V-cycle (k_mg_post on the finest level).
-__global__ void k_init_mg(const double *b, double *x, double *r, double *partial, long long n) {
+template <class T>
+__global__ void k_init_mg(const T *b, T *x, T *r, double *partial, long long n) {
     __shared__ double sh[32];
     double rr = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-        const double rv = b[s];
+        const T rv = b[s];
         x[s] = 0;
         r[s] = rv;
-        rr += rv * rv;
+        rr += double(rv) * double(rv);
     }
     rr = block_sum(rr, sh);
     if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = rr;
 }
 
-__global__ void k_update_mg(double *x, double *r, const double *p, const double *q, const double *scal,
-                            double *partial, long long n) {
+template <class T>
+__global__ void k_update_mg(T *x, T *r, const T *p, const T *q, const double *scal, double *partial, long long n) {
     __shared__ double sh[32];
-    const double alpha = scal[S_ALPHA];
+    const T alpha = T(scal[S_ALPHA]);
     double rr = 0;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
         x[s] += alpha * p[s];
-        const double rv = r[s] - alpha * q[s];
+        const T rv = r[s] - alpha * q[s];
         r[s] = rv;
-        rr += rv * rv;
+        rr += double(rv) * double(rv);
     }
     rr = block_sum(rr, sh);
     if (threadIdx.x == 0) partial[gridDim.x + blockIdx.x] = rr;
@@ -508,41 +528,45 @@ namespace {
 
 constexpr int MG_MAX_LEV = 16;
 
+template <class T>
 struct MgPlan {
-    int L = 0;                     // coarse levels 1..L (level L is the coarsest)
-    MgLevel lev[MG_MAX_LEV + 1];   // lev[0]: the fine level (n only)
-    double *cinv = nullptr;        // coarsest dense inverse
-    int *flag = nullptr;           // coarse-row overflow
+    int L = 0;                        // coarse levels 1..L (level L is the coarsest)
+    MgLevelT<T> lev[MG_MAX_LEV + 1];  // lev[0]: the fine level (n only)
+    double *cinv = nullptr;           // coarsest dense inverse
+    int *flag = nullptr;              // coarse-row overflow
 };
 
 // Carves the levels of an n-row solve out of `base` (null: sizes only);
 // returns the doubles used.
-size_t mg_plan(long long n, int cap, double *base, MgPlan &pl) {
+template <class T>
+size_t mg_plan(long long n, int cap, double *base, MgPlan<T> &pl) {
     auto pad = [](size_t k) { return (k + 31) & ~size_t(31); };
     size_t used = 0;
-    auto take = [&](size_t doubles) {
-        double *p = base ? base + used : nullptr;
-        used += pad(doubles);
+    // room for `count` elements of type E, in doubles
+    auto take = [&](size_t count, auto *type) {
+        using E = std::remove_pointer_t<decltype(type)>;
+        E *p = base ? reinterpret_cast<E *>(base + used) : nullptr;
+        used += pad((count * sizeof(E) + sizeof(double) - 1) / sizeof(double));
         return p;
     };
-    pl = MgPlan{};
+    pl = MgPlan<T>{};
     pl.lev[0].n = n;
     long long m = n;
     while (m > MG_COARSE && pl.L < MG_MAX_LEV) {
         m = (m + MG_B - 1) / MG_B;
-        MgLevel &v = pl.lev[++pl.L];
+        MgLevelT<T> &v = pl.lev[++pl.L];
         v.n = m;
-        v.val = take(size_t(cap) * m);
-        v.dinv = take(m);
-        v.r = take(m);
-        v.z = take(m);
-        v.zo = take(m);
-        v.cnt = reinterpret_cast<int *>(take((m + 1) / 2));
-        v.col = reinterpret_cast<int *>(take((size_t(cap) * m + 1) / 2));
+        v.val = take(size_t(cap) * m, (T *)nullptr);
+        v.dinv = take(m, (T *)nullptr);
+        v.r = take(m, (T *)nullptr);
+        v.z = take(m, (T *)nullptr);
+        v.zo = take(m, (T *)nullptr);
+        v.cnt = take(m, (int *)nullptr);
+        v.col = take(size_t(cap) * m, (int *)nullptr);
     }
     if (pl.L > 0) {
-        pl.cinv = take(size_t(MG_COARSE) * MG_COARSE);
-        pl.flag = reinterpret_cast<int *>(take(1));
+        pl.cinv = take(size_t(MG_COARSE) * MG_COARSE, (double *)nullptr);
+        pl.flag = take(1, (int *)nullptr);
     }
     return used;
 }
@@ -552,30 +576,31 @@ int coarse_grid(long long n) {
     return int(g < 148 * 8 ? (g < 1 ? 1 : g) : 148 * 8);
 }
 
-EllView ell(const MgLevel &v) { return EllView{v.cnt, v.col, v.val, v.n}; }
+template <class T>
+EllViewT<T> ell(const MgLevelT<T> &v) { return EllViewT<T>{v.cnt, v.col, v.val, v.n}; }
 
 // Builds the coarse levels of A; false when a coarse row outgrew MG_CAP.
-template <class M, int SLOTS>
-void mg_coarsen_all(const M &A, long long gauge, const double *scal, const MgPlan &pl, cudaStream_t st) {
+template <class M, int SLOTS, class T>
+void mg_coarsen_all(const M &A, long long gauge, const double *scal, const MgPlan<T> &pl, cudaStream_t st) {
     for (int l = 1; l <= pl.L; ++l) {
         const int g = coarse_grid(32 * pl.lev[l].n);  // one warp per coarse row
         if (l == 1)
-            k_mg_coarsen<M, SLOTS><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
+            k_mg_coarsen<M, SLOTS, T><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
         else
-            k_mg_coarsen<EllView, SLOTS><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal, pl.lev[l],
-                                                          pl.flag);
+            k_mg_coarsen<EllViewT<T>, SLOTS, T><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal,
+                                                                  pl.lev[l], pl.flag);
         note_launch();
     }
 }
 
-template <class M>
-bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan &pl, int cap, cudaStream_t st) {
+template <class M, class T>
+bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan<T> &pl, int cap, cudaStream_t st) {
     SDOT_CUDA(cudaMemsetAsync(pl.flag, 0, sizeof(int), st));
     if (cap > 64)
         mg_coarsen_all<M, 4>(A, gauge, scal, pl, st);
     else
         mg_coarsen_all<M, 2>(A, gauge, scal, pl, st);
-    k_mg_coarsest_setup<<<1, MG_COARSE, 0, st>>>(ell(pl.lev[pl.L]), int(pl.lev[pl.L].n), pl.cinv);
+    k_mg_coarsest_setup<T><<<1, MG_COARSE, 0, st>>>(ell(pl.lev[pl.L]), int(pl.lev[pl.L].n), pl.cinv);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
     int flag = 0;
@@ -586,59 +611,65 @@ bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan &pl,
 
 // z0 = V-cycle(r0) on the finest level (pre-smoothed values in zpre0), with
 // r0 . z0 per block into partial[0 .. g) and, when p0 is given, p0 = z0.
-template <class M>
-void mg_vcycle(const M &A, long long gauge, const double *scal, const double *dinv0, const MgPlan &pl,
-               const double *r0, double *zpre0, double *z0, double *partial, double *p0, int g, cudaStream_t st) {
+template <class M, class T>
+void mg_vcycle(const M &A, long long gauge, const double *scal, const T *dinv0, const MgPlan<T> &pl, const T *r0,
+               T *zpre0, T *z0, double *partial, T *p0, int g, cudaStream_t st) {
     const long long n = pl.lev[0].n;
-    k_mg_pre<M><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].r);
+    k_mg_pre<M, T><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].r);
     for (int l = 1; l < pl.L; ++l) {
-        const MgLevel &v = pl.lev[l];
-        k_mg_pre<EllView><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z, pl.lev[l + 1].r);
+        const MgLevelT<T> &v = pl.lev[l];
+        k_mg_pre<EllViewT<T>, T><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
+                                                                   pl.lev[l + 1].r);
     }
-    const MgLevel &c = pl.lev[pl.L];
-    k_mg_coarsest_apply<<<1, MG_COARSE, 0, st>>>(pl.cinv, int(c.n), c.r, c.zo);
+    const MgLevelT<T> &c = pl.lev[pl.L];
+    k_mg_coarsest_apply<T><<<1, MG_COARSE, 0, st>>>(pl.cinv, int(c.n), c.r, c.zo);
     for (int l = pl.L - 1; l >= 1; --l) {
-        const MgLevel &v = pl.lev[l];
-        k_mg_post<EllView, false><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
-                                                                   pl.lev[l + 1].zo, v.zo, nullptr, nullptr);
+        const MgLevelT<T> &v = pl.lev[l];
+        k_mg_post<EllViewT<T>, false, T><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
+                                                                           pl.lev[l + 1].zo, v.zo, nullptr, nullptr);
     }
-    k_mg_post<M, true><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].zo, z0, partial, p0);
+    k_mg_post<M, true, T><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].zo, z0, partial, p0);
 }
 
-int mg_launches(const MgPlan &pl) { return 2 * pl.L + 1; }
+template <class T>
+int mg_launches(const MgPlan<T> &pl) { return 2 * pl.L + 1; }
 
 }  // namespace
 
 size_t mg_work_doubles(long long n, int cap) {
-    MgPlan pl;
+    MgPlan<double> pl;
     return mg_plan(n, cap, nullptr, pl);
 }
 
-void pcg_bind(PcgWork &w, double *base, long long n) {
+template <class T>
+void pcg_bind(PcgWorkT<T> &w, double *base, long long n) {
     const long long m = n + 32;
-    w.r = base;
-    w.z = base + m;
-    w.p = base + 2 * m;
-    w.q = base + 3 * m;
-    w.dinv = base + 4 * m;
-    w.partial = base + 5 * m;
+    T *v = reinterpret_cast<T *>(base);
+    w.r = v;
+    w.z = v + m;
+    w.p = v + 2 * m;
+    w.q = v + 3 * m;
+    w.dinv = v + 4 * m;
+    w.partial = base + (5 * m * (long long)sizeof(T) + 7) / 8;
     w.scal = w.partial + 6 * PCG_BLOCKS;
 }
+template void pcg_bind<double>(PcgWorkT<double> &, double *, long long);
+template void pcg_bind<float>(PcgWorkT<float> &, double *, long long);
 
 namespace {
 
-template <class M>
-PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
-                  int max_iter, const PcgWork &w, cudaStream_t st, int check, bool graph, bool multilevel) {
+template <class M, class T>
+PcgResult pcg_run(const M &A, long long n, long long gauge_row, const T *b, T *x, double rel_tol, int max_iter,
+                  const PcgWorkT<T> &w, cudaStream_t st, int check, bool graph, bool multilevel) {
     PcgResult res;
     if (n <= 0) {
         res.converged = true;
         return res;
     }
     const int g = grid_of(n);
-    k_diag_inv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.dinv, w.scal);
+    k_diag_inv<M, T><<<g, TB, 0, st>>>(A, n, gauge_row, w.dinv, w.scal);
     note_launch();
-    MgPlan pl;
+    MgPlan<T> pl;
     const int cap = w.mg_cap > 64 ? MG_CAP_MAX : 64;
     bool mg = multilevel && n > MG_COARSE && w.mg && mg_plan(n, cap, nullptr, pl) <= w.mg_doubles;
     if (mg) {
@@ -646,12 +677,12 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
         mg = mg_setup(A, gauge_row, w.scal, pl, cap, st);
     }
     if (mg) {
-        k_init_mg<<<g, TB, 0, st>>>(b, x, w.r, w.partial, n);
+        k_init_mg<T><<<g, TB, 0, st>>>(b, x, w.r, w.partial, n);
         mg_vcycle(A, gauge_row, w.scal, w.dinv, pl, w.r, w.q, w.z, w.partial, w.p, g, st);
         for (int c = 0; c < 1 + mg_launches(pl); ++c) note_launch();
         res.levels = pl.L;
     } else {
-        k_init<<<g, TB, 0, st>>>(b, x, w.r, w.z, w.p, w.dinv, w.partial, n);
+        k_init<T><<<g, TB, 0, st>>>(b, x, w.r, w.z, w.p, w.dinv, w.partial, n);
         note_launch();
     }
     k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 0);
@@ -668,17 +699,17 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
     const double target = rel_tol * rel_tol * rr0;
     auto launch_chunk = [&](int chunk) {
         for (int c = 0; c < chunk; ++c) {
-            k_spmv<M><<<g, TB, 0, st>>>(A, n, gauge_row, w.p, w.q, w.scal, w.partial);
+            k_spmv<M, T><<<g, TB, 0, st>>>(A, n, gauge_row, w.p, w.q, w.scal, w.partial);
             k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 1);
             if (mg) {
                 // q is free once r is updated: it holds the pre-smoothed values
-                k_update_mg<<<g, TB, 0, st>>>(x, w.r, w.p, w.q, w.scal, w.partial, n);
-                mg_vcycle(A, gauge_row, w.scal, w.dinv, pl, w.r, w.q, w.z, w.partial, nullptr, g, st);
+                k_update_mg<T><<<g, TB, 0, st>>>(x, w.r, w.p, w.q, w.scal, w.partial, n);
+                mg_vcycle(A, gauge_row, w.scal, w.dinv, pl, w.r, w.q, w.z, w.partial, (T *)nullptr, g, st);
             } else {
-                k_update<<<g, TB, 0, st>>>(x, w.r, w.z, w.p, w.q, w.dinv, w.scal, w.partial, n);
+                k_update<T><<<g, TB, 0, st>>>(x, w.r, w.z, w.p, w.q, w.dinv, w.scal, w.partial, n);
             }
             k_final<<<1, TB, 0, st>>>(w.partial, g, w.scal, 2);
-            k_pupdate<<<g, TB, 0, st>>>(w.z, w.p, w.scal, n);
+            k_pupdate<T><<<g, TB, 0, st>>>(w.z, w.p, w.scal, n);
         }
     };
     const int per_iter = 5 + (mg ? mg_launches(pl) : 0);
@@ -731,7 +762,7 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const double *b,
 
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
                     int max_iter, const PcgWork &w, cudaStream_t st, int check, bool graph, bool multilevel) {
-    return pcg_run(RowsMat{rows}, n, gauge_row, b, x, rel_tol, max_iter, w, st, check, graph, multilevel);
+    return pcg_run(rows_mat(rows), n, gauge_row, b, x, rel_tol, max_iter, w, st, check, graph, multilevel);
 }
 
 PcgResult pcg_solve_csr(const CsrMat &A, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
@@ -765,6 +796,146 @@ void gather_sorted(const double *t_orig, const int *idx, double *t_sorted, long 
     k_gather_sorted<<<grid_of(n), TB, 0, st>>>(t_orig, idx, t_sorted, n);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
+}
+
+// ---- FP32 solves with FP64 iterative refinement ---------------------------
+namespace {
+
+__global__ void k_rows_to_float(Rows R, long long n, float *val32, float *side32, const unsigned long long *side_used) {
+    const long long total = (long long)R.cap * R.stride;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+        if (i % R.stride < n) val32[i] = float(R.val[i]);
+    const long long ns = side_used ? (long long)*side_used : 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns && i < R.side_cap;
+         i += (long long)gridDim.x * blockDim.x)
+        side32[i] = float(R.side_val[i]);
+}
+
+// partial[block] = sum of v^2 over the block's entries
+__global__ void k_sumsq(const double *v, long long n, double *partial) {
+    __shared__ double sh[32];
+    double a = 0;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
+        a += v[s] * v[s];
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = a;
+}
+__global__ void k_sum_partials(const double *partial, int nb, double *out) {
+    __shared__ double sh[32];
+    double a = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) a += partial[i];
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) *out = a;
+}
+// out32 = scale * r (rounded to float)
+__global__ void k_to_float(const double *r, double scale, float *out32, long long n) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
+        out32[s] = float(scale * r[s]);
+}
+// x += scale * d (d in float or double)
+template <class T>
+__global__ void k_add_scaled(double *x, const T *d, double scale, long long n) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x)
+        x[s] += scale * double(d[s]);
+}
+// r = b - (H + gauge term) x, in FP64
+template <class M>
+__global__ void k_residual(M A, long long n, long long g, const double *scal, const double *b, const double *x,
+                           double *r) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        double v = A.row_dot(s, x);
+        if (s == g) v += scal[S_GDIAG] * x[s];
+        r[s] = b[s] - v;
+    }
+}
+
+double sumsq(const double *v, long long n, double *partial, double *dev_out, cudaStream_t st) {
+    const int g = grid_of(n);
+    k_sumsq<<<g, TB, 0, st>>>(v, n, partial);
+    k_sum_partials<<<1, TB, 0, st>>>(partial, g, dev_out);
+    note_launch();
+    note_launch();
+    double h = 0;
+    SDOT_CUDA(cudaMemcpyAsync(&h, dev_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SDOT_CUDA(cudaStreamSynchronize(st));
+    return h;
+}
+
+}  // namespace
+
+void rows_to_float(const Rows &rows, long long n, float *val32, float *side_val32, cudaStream_t st) {
+    if (n <= 0) return;
+    k_rows_to_float<<<PCG_BLOCKS, TB, 0, st>>>(rows, n, val32, side_val32, rows.side_used);
+    note_launch();
+    SDOT_CUDA(cudaGetLastError());
+}
+
+PcgResult pcg_solve_refined(const Rows &rows, const float *val32, const float *side_val32, long long n,
+                            long long gauge_row, const double *b, double *x, double rel_tol, int max_iter,
+                            const PcgWork &w64, const PcgWorkT<float> &w32, double *res64, cudaStream_t st,
+                            double inner_tol, int check, bool multilevel) {
+    PcgResult res;
+    if (n <= 0) {
+        res.converged = true;
+        return res;
+    }
+    const RowsMat A64 = rows_mat(rows);
+    const RowsMatT<float> A32{rows, val32, side_val32};
+    const int g = grid_of(n);
+    double *r64 = res64;                                        // n doubles: the FP64 residual
+    float *b32 = reinterpret_cast<float *>(res64 + n);          // n floats: the scaled residual
+    float *d32 = b32 + n;                                       // n floats: the FP32 correction
+    double *e64 = res64 + n;                                    // n doubles (FP64 fallback, reuses b32 / d32)
+    double *dev_sum = w64.scal + S_NSCAL;                       // a spare device scalar
+    // the FP64 gauge term (scal[S_GDIAG]) for the residuals
+    k_diag_inv<RowsMat, double><<<g, TB, 0, st>>>(A64, n, gauge_row, w64.dinv, w64.scal);
+    note_launch();
+    SDOT_CUDA(cudaMemsetAsync(x, 0, size_t(n) * sizeof(double), st));
+    SDOT_CUDA(cudaMemcpyAsync(r64, b, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const double bb = sumsq(b, n, w64.partial, dev_sum, st);
+    if (!(bb > 0)) {
+        res.converged = bb == 0;
+        return res;
+    }
+    const double target = rel_tol * rel_tol * bb;
+    double rr = bb;
+    int it = 0;
+    bool fp32_ok = true;
+    for (int outer = 0; outer < 60 && it < max_iter; ++outer) {
+        if (rr <= target) break;
+        const double nr = std::sqrt(rr);
+        if (fp32_ok) {
+            // the correction for the current residual, solved in FP32
+            k_to_float<<<g, TB, 0, st>>>(r64, 1.0 / nr, b32, n);
+            note_launch();
+            const PcgResult in = pcg_run(A32, n, gauge_row, b32, d32, inner_tol, std::min(max_iter - it, 4000), w32,
+                                         st, check, st != nullptr, multilevel);
+            it += in.iterations;
+            res.levels = in.levels;
+            k_add_scaled<float><<<g, TB, 0, st>>>(x, d32, nr, n);
+        } else {
+            // the rest in FP64: solve H e = r, x += e
+            const PcgResult in = pcg_run(A64, n, gauge_row, r64, e64, std::sqrt(target / rr), max_iter - it, w64,
+                                         st, check, st != nullptr, multilevel);
+            it += in.iterations;
+            res.levels = in.levels;
+            k_add_scaled<double><<<g, TB, 0, st>>>(x, e64, 1.0, n);
+        }
+        note_launch();
+        k_residual<RowsMat><<<g, TB, 0, st>>>(A64, n, gauge_row, w64.scal, b, x, r64);
+        note_launch();
+        SDOT_CUDA(cudaGetLastError());
+        const double rr_new = sumsq(r64, n, w64.partial, dev_sum, st);
+        if (!(rr_new == rr_new)) break;
+        // an outer step that does not halve |r|: the FP32 matrix is too far
+        // from H for this system
+        if (fp32_ok && !(rr_new <= 0.25 * rr)) fp32_ok = false;
+        rr = rr_new;
+    }
+    res.iterations = it;
+    res.rel_residual = std::sqrt(rr / bb);
+    res.converged = rr <= target;
+    return res;
 }
 
 }  // namespace sdot

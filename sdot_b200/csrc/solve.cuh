@@ -12,21 +12,27 @@
 namespace sdot {
 
 // Scratch of one PCG solve over n rows (device buffers owned by the caller).
-struct PcgWork {
-    double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
+// T: the precision of the vectors and of the matrix values (double, or float
+// for the inner solves of the iterative refinement); the scalars of the
+// iteration and every reduction stay in double.
+template <class T>
+struct PcgWorkT {
+    T *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
     double *partial = nullptr;  // PCG_BLOCKS partial sums (x 2)
     double *scal = nullptr;     // device scalars (see solve.cu)
     double *mg = nullptr;       // multilevel storage (mg_work_doubles(n, mg_cap) doubles), or null
     size_t mg_doubles = 0;
     int mg_cap = 64;            // coarse row width: 64 or 128 (3D)
 };
+using PcgWork = PcgWorkT<double>;
 
 // One coarse level of the multilevel preconditioner (device arrays).
-struct MgLevel {
+template <class T>
+struct MgLevelT {
     long long n = 0;
     int *cnt = nullptr, *col = nullptr;  // ELL rows (width PcgWork::mg_cap)
-    double *val = nullptr, *dinv = nullptr;
-    double *r = nullptr, *z = nullptr, *zo = nullptr;  // right-hand side, smoothed, output
+    T *val = nullptr, *dinv = nullptr;
+    T *r = nullptr, *z = nullptr, *zo = nullptr;  // right-hand side, smoothed, output
 };
 
 // Doubles of multilevel storage a solve over n rows needs (coarse rows of
@@ -35,7 +41,8 @@ size_t mg_work_doubles(long long n, int cap);
 constexpr int PCG_BLOCKS = 148 * 4;
 
 size_t pcg_work_doubles(long long n);
-void pcg_bind(PcgWork &w, double *base, long long n);
+template <class T>
+void pcg_bind(PcgWorkT<T> &w, double *base, long long n);
 
 struct PcgResult {
     int iterations = 0;
@@ -58,6 +65,22 @@ struct PcgResult {
 PcgResult pcg_solve(const Rows &rows, long long n, long long gauge_row, const double *b, double *x, double rel_tol,
                     int max_iter, const PcgWork &w, cudaStream_t st, int check = 32, bool graph = false,
                     bool multilevel = false);
+
+// The same system solved by iterative refinement: each outer step solves
+// H d = r for the current FP64 residual r (scaled to unit norm) by PCG in FP32
+// on an FP32 copy of the rows' values (val32 / side_val32: same layout as
+// rows.val / rows.side_val; see rows_to_float), to the relative tolerance
+// inner_tol, adds d to x in FP64 and recomputes r = b - H x with the FP64
+// rows.  Stops at |r| <= rel_tol |b|.  An outer step that does not halve |r|
+// (the FP32 matrix too far from H for this system) hands the rest of the
+// solve to the FP64 PCG.  Iterations of both kinds are counted.
+PcgResult pcg_solve_refined(const Rows &rows, const float *val32, const float *side_val32, long long n,
+                            long long gauge_row, const double *b, double *x, double rel_tol, int max_iter,
+                            const PcgWork &w64, const PcgWorkT<float> &w32, double *res64, cudaStream_t st,
+                            double inner_tol = 1e-5, int check = 32, bool multilevel = true);
+// FP32 copies of the rows' values (ELL slots of the first n rows and the side
+// buffer's side_used entries).
+void rows_to_float(const Rows &rows, long long n, float *val32, float *side_val32, cudaStream_t st);
 
 // The same solve on a CSR matrix (device arrays: off[n + 1], col[nnz], val[nnz]).
 struct CsrMat {

@@ -220,17 +220,22 @@ class PowerDiagram:
         return out
 
     def solve_weights(self, target_masses, rel_mass_tol=1e-10, max_iter=150, damping=True, pcg_rel_tol=1e-12,
-                      pcg_max_iter=20000, verbosity=0, preconditioner="multilevel"):
+                      pcg_max_iter=20000, verbosity=0, preconditioner="multilevel", linear_solver=None):
         """Newton on the weights so that every cell mass reaches its target
         (OptimalTransportSolver::solve, OptimalTransportSolver.tcc:27-119).
         Updates the weights of this diagram and returns the solver report as
         a dict; raises SdotError when the tolerance is not reached.
         preconditioner: "multilevel" (V-cycle over Morton aggregates) or
-        "jacobi"."""
+        "jacobi".  linear_solver: "fp64" (FP64 PCG) or "fp32_refined" (FP32
+        PCG with FP64 iterative refinement); by default "fp32_refined" for a
+        mixed-precision diagram and "fp64" otherwise."""
         t = _f64(target_masses, (self.nb_diracs,))
+        if linear_solver is None:
+            linear_solver = "fp32_refined" if self.precision == "mixed" else "fp64"
         opt = _lib.SdotNewtonOptions(int(max_iter), float(rel_mass_tol), int(pcg_max_iter), float(pcg_rel_tol),
                                      int(bool(damping)), int(verbosity),
-                                     {"multilevel": 0, "jacobi": 1}[preconditioner])
+                                     {"multilevel": 0, "jacobi": 1}[preconditioner],
+                                     {"fp64": 0, "fp32_refined": 1}[linear_solver])
         rep = _lib.SdotNewtonReport()
         st = self._lib.sdot_solve(self._ctx, _ptr(t), SDOT_HOST, ctypes.byref(opt), ctypes.byref(rep))
         w = np.empty(self.nb_diracs)

@@ -184,3 +184,80 @@ def test_multilevel_newton_mirrored_clusters(gpu_lib):
     m = g.integrals()
     assert np.max(np.abs(m - t) / t) <= 1e-8
     assert rep["pcg_levels"] >= 4
+
+
+# ---- FP32 PCG with FP64 iterative refinement (linear_solver="fp32_refined"):
+# the residuals and the weights stay FP64, so the solve reaches the same
+# tolerance and Newton the same weights as with the FP64 PCG
+def solve_gpu(p, w0, target, linear_solver, tol, radial_func="unit", image=None):
+    from sdot_b200.power_diagram import PowerDiagram
+
+    g = PowerDiagram(p, w0, radial_func=radial_func)
+    if image is not None:
+        g.set_image_density(image)
+    else:
+        g.add_box_shape(np.zeros(p.shape[1]), np.ones(p.shape[1]))
+    rep = g.solve_weights(target, rel_mass_tol=tol, linear_solver=linear_solver)
+    return g, g.get_weights(), rep
+
+
+def test_refined_newton_config1_vs_oracle(gpu_lib, ref_oracle):
+    c = workloads.config1()
+    n = len(c["weights"])
+    t = np.full(n, 1.0 / n)
+    g, w_g, rep = solve_gpu(c["positions"], c["weights"], t, "fp32_refined", 1e-12)
+    ref = ref_oracle.RefPowerDiagram(c["positions"], c["weights"])
+    ref.add_box_shape([0.0, 0.0], [1.0, 1.0])
+    w_r, rep_r = newton.solve(ref, t, c["weights"], tol=1e-12)
+    assert rep["max_rel_mass_error"] <= 1e-12
+    check_weights(w_g, w_r)
+
+
+def test_refined_csr_solve_matches_fp64(gpu_lib):
+    # one linear solve: refined vs FP64 PCG on the same right-hand side, both
+    # to a relative residual of 1e-12 (through the Newton step of C1 at w = 0)
+    c = workloads.config1()
+    n = len(c["weights"])
+    ws = {}
+    for ls in ("fp64", "fp32_refined"):
+        g, w, rep = solve_gpu(c["positions"], np.zeros(n), c["target"], ls, 1e-11)
+        ws[ls] = (w, rep)
+    assert np.abs(ws["fp64"][0] - ws["fp32_refined"][0]).max() <= 1e-9 * np.abs(ws["fp64"][0]).max()
+    assert ws["fp32_refined"][1]["iterations"] <= ws["fp64"][1]["iterations"] + 1
+
+
+def test_refined_newton_disc_clip_image(gpu_lib, ref_oracle):
+    c = workloads.config3(n=4000, res=64)
+    n = len(c["weights"])
+    g, w_g, rep = solve_gpu(c["positions"], c["weights"], c["target"], "fp32_refined", 1e-12,
+                            radial_func="in_ball_w05", image=c["image"])
+    ref = ref_oracle.RefPowerDiagram(c["positions"], c["weights"], radial_func="in_ball_w05")
+    ref.set_image_density(c["image"])
+    w_r, rep_r = newton.solve(ref, c["target"], c["weights"], tol=1e-12, ball_cut=True)
+    assert rep_r["converged"]
+    check_weights(w_g, w_r)
+
+
+def test_refined_newton_mirrored_clusters(gpu_lib):
+    rng = np.random.default_rng(53)
+    n = 300_000
+    p = np.concatenate([rng.random((n // 2, 2)), workloads.clustered_points(n - n // 2, 2, rng, boundary="reflect")])
+    t = np.full(n, 1.0 / n)
+    g, w, rep = solve_gpu(p, np.zeros(n), t, "fp32_refined", 1e-8)
+    m = g.integrals()
+    assert np.max(np.abs(m - t) / t) <= 1e-8
+
+
+def test_refined_newton_3d(gpu_lib):
+    from sdot_b200.power_diagram import PowerDiagram
+
+    c = workloads.config4(n=20_000)
+    n = len(c["weights"])
+    out = {}
+    for ls in ("fp64", "fp32_refined"):
+        g = PowerDiagram(c["positions"], c["weights"])
+        g.add_box_shape([0, 0, 0], [1, 1, 1])
+        g.set_polynomial_density(c["density"])
+        g.solve_weights(c["target"], rel_mass_tol=1e-10, linear_solver=ls)
+        out[ls] = g.get_weights()
+    assert np.abs(out["fp64"] - out["fp32_refined"]).max() <= 1e-8 * np.abs(out["fp64"]).max()
