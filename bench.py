@@ -45,9 +45,20 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Laguerre cells/s (areas + centroids + CSR Hessian), 2D, 1M Diracs"
 UNIT = "cells/s"
-# Algorithmic work per cell (reference algorithm counts on 2D uniform inputs,
-# FMA = 2 flops): 22.8 cut attempts x (12 + 5 x 5.42 vertices)
-# + 38.1 boxes x 6 vertices x 12 + 6 final vertices x 35 = 3.9 kflop.
+# Algorithmic work per cell of the 2D workload: the operation count of the
+# reference algorithm (FMA = 2 flops; 12 per cut attempt, 5 per vertex per
+# attempt, 12 per vertex per eviction test, 35 per final vertex) with the
+# counts measured on the benchmark input by the counting build
+# (tests/count_work.py -> profiles/work_counts_c2_1M.json); 3.9 kflop, the
+# count on uniform inputs, when that file is absent.
+def flops_per_cell_2d():
+    try:
+        with open(os.path.join(ROOT, "profiles", "work_counts_c2_1M.json")) as f:
+            return float(json.load(f)["flops_per_cell"]), "measured on the benchmark input (tests/count_work.py)"
+    except (OSError, KeyError, ValueError):
+        return 3.9e3, "uniform-input count (the benchmark input's count is absent)"
+
+
 FLOPS_PER_CELL = 3.9e3
 # per-cell algorithmic HBM bytes: positions + weight in (24), area (8),
 # centroid (16), ~7 Hessian entries x 12 + offset 8
@@ -260,7 +271,10 @@ def run_ours(args):
     c = workload(args.n, rank, args.config)
     n = args.n
     dim = 3 if args.config == "c4" else 2
-    flops_cell, bytes_cell = (FLOPS_PER_CELL_3D, BYTES_PER_CELL_3D) if dim == 3 else (FLOPS_PER_CELL, BYTES_PER_CELL)
+    if dim == 3:
+        flops_cell, bytes_cell, flops_src = FLOPS_PER_CELL_3D, BYTES_PER_CELL_3D, "3D uniform-input count"
+    else:
+        (flops_cell, flops_src), bytes_cell = flops_per_cell_2d(), BYTES_PER_CELL
     pos_h = torch.from_numpy(np.ascontiguousarray(c["positions"])).pin_memory()
     w_h = torch.from_numpy(np.ascontiguousarray(c["weights"])).pin_memory()
     pos_d = pos_h.to(dev)
@@ -387,7 +401,7 @@ def run_ours(args):
     roofline = {"bound": "fp64", "kernel": kern, "achieved": achieved,
                 "peak": float(peaks[0]), "unit": "TFLOP/s", "frac": achieved / float(peaks[0]) if peaks[0] else None,
                 "traffic": traffic, "algorithmic_bytes_per_launch": bytes_cell * n,
-                "flops_per_cell": flops_cell, "cell_kernel_ms": cell,
+                "flops_per_cell": flops_cell, "flops_per_cell_source": flops_src, "cell_kernel_ms": cell,
                 "peak_source": "FP64 FMA peak measured in this run by sdot_measure_fma_peaks (FMA-only kernel); "
                                "the path uses no tensor cores and its HBM floor is far below the FP64 one",
                 "hbm_view": {"achieved_gbs": bytes_cell * n / (cell * 1e-3) / 1e9, "peak_gbs": hbm_peak(),
@@ -464,39 +478,59 @@ def mixed_leg(L, c, n, dev, flush, steps):
 
 
 def newton_leg():
-    """Newton times from w = 0, damped, FP64, multilevel-preconditioned CG:
-    C1 (10k uniform) to 1e-10.  The 1M clustered mix cannot reach 1e-8 in
-    FP64: clamping puts pairs of Diracs 4e-8 apart on the box edges, and
-    the damped Newton stalls at a relative mass error of 3.2e-4 (the compiled
-    reference with a direct solve stalls the same way, at 1.5e-6 already at
-    300k), so it runs to 1e-3; with the clustered Diracs mirrored at the
-    faces instead, the closest pairs (~3e-7 apart) leave a floor of 2.3e-8,
-    so that mix runs to 1e-7."""
+    """Newton times (damped, multilevel-preconditioned CG) from the
+    configured starting weights, with FP64 PCG and with FP32 PCG + FP64
+    iterative refinement:
+      C1  10k uniform, w = 0, to 1e-10;
+      C2  the 1M clustered mix from w = 0: clamping puts pairs of Diracs
+          4e-8 apart on the box edges, and FP64 cannot reach 1e-8 there (the
+          compiled reference with a direct solve stalls at 3.6e-7 at 100k,
+          tests/golden/newton_floor_c2.json), so the clamped mix runs to 1e-3
+          and the same mix with the clustered Diracs mirrored at the faces
+          (closest pairs ~3e-7 apart) to 1e-7;
+      C3  500k, 512^2 image, disc clip, w0 = (0.5/sqrt n)^2, targets 0.8/n, to 1e-8;
+      C4  200k 3D mix, density (1 + 0.3 xyz) normalised, w = 0, to 1e-8."""
     from sdot_b200 import workloads
     from sdot_b200.power_diagram import PowerDiagram
 
     c2 = workloads.config2()
-    rng = np.random.Generator(np.random.PCG64(workloads.SEED0 + 2))
+    rng = np.random.default_rng(workloads.SEED0 + 2)
     n2 = len(c2["weights"])
     mirrored = np.concatenate([workloads.uniform_points(n2 // 2, 2, rng),
                                workloads.clustered_points(n2 - n2 // 2, 2, rng, boundary="reflect")])
+    c3 = workloads.config3()
+    c4 = workloads.config4()
+    cases = [("C1_10k_to_1e-10", workloads.config1()["positions"], None, 1e-10, {}),
+             ("C2_1M_clamped_from_w0_to_1e-3", c2["positions"], None, 1e-3, {}),
+             ("C2_1M_mirrored_from_w0_to_1e-7", mirrored, None, 1e-7, {}),
+             ("C3_500k_image_disc_to_1e-8", c3["positions"], c3["weights"], 1e-8,
+              {"image": c3["image"], "target": c3["target"], "radial_func": "in_ball_w05"}),
+             ("C4_200k_3d_to_1e-8", c4["positions"], None, 1e-8, {"density": c4["density"]})]
     out = {}
-    for name, pos, tol in (("C1_10k_to_1e-10", workloads.config1()["positions"], 1e-10),
-                           ("C2_1M_clamped_from_w0_to_1e-3", c2["positions"], 1e-3),
-                           ("C2_1M_mirrored_from_w0_to_1e-7", mirrored, 1e-7)):
-        n = len(pos)
-        g = PowerDiagram(pos, np.zeros(n))
-        g.add_box_shape([0, 0], [1, 1])
-        t0 = time.perf_counter()
-        try:
-            rep = g.solve_weights(np.full(n, 1.0 / n), rel_mass_tol=tol)
-        except Exception as e:
-            out[name] = {"error": str(e), "time_s": time.perf_counter() - t0}
-            continue
-        wall = time.perf_counter() - t0
-        out[name] = {"time_s": wall, "iterations": rep["iterations"], "pcg_iterations": int(rep["pcg_iterations"]),
-                     "pcg_levels": rep["pcg_levels"], "evaluations": rep["evaluations"],
-                     "max_rel_mass_error": rep["max_rel_mass_error"]}
+    for name, pos, w0, tol, extra in cases:
+        n, dim = pos.shape
+        for ls in ("fp64", "fp32_refined"):
+            if name.startswith("C2_1M_clamped") and ls != "fp64":
+                continue
+            g = PowerDiagram(pos, np.zeros(n) if w0 is None else w0, radial_func=extra.get("radial_func", "unit"))
+            if "image" in extra:
+                g.set_image_density(extra["image"])
+            else:
+                g.add_box_shape(np.zeros(dim), np.ones(dim))
+            if "density" in extra:
+                g.set_polynomial_density(extra["density"])
+            t = extra.get("target", np.full(n, 1.0 / n))
+            key = f"{name}_{ls}"
+            t0 = time.perf_counter()
+            try:
+                rep = g.solve_weights(t, rel_mass_tol=tol, linear_solver=ls)
+            except Exception as e:
+                out[key] = {"error": str(e), "time_s": time.perf_counter() - t0}
+                continue
+            wall = time.perf_counter() - t0
+            out[key] = {"time_s": wall, "iterations": rep["iterations"], "pcg_iterations": int(rep["pcg_iterations"]),
+                        "pcg_levels": rep["pcg_levels"], "evaluations": rep["evaluations"],
+                        "max_rel_mass_error": rep["max_rel_mass_error"]}
     return out
 
 

@@ -316,6 +316,13 @@ int sdot_measure_fma_peaks(double *tflops2);
  * assembly (out6[3..5]).  Release builds report zeros.                       */
 int sdot_debug_checks(uint64_t *out6);
 
+/* Counting builds (-DSDOT_COUNT) only: the work of the 2D fast tier's walks
+ * since the last reset: out8[0] cut attempts, [1] vertices classified at
+ * them, [2] node (eviction) tests, [3] vertices tested at them, [4] effective
+ * cuts, [5] final vertices, [6] cells.  The operands of the operation count
+ * of the roofline.  Release builds report zeros.  No reference counterpart. */
+int sdot_debug_work_counts(uint64_t *out8, int reset);
+
 #ifdef __cplusplus
 }
 #endif

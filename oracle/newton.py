@@ -30,9 +30,10 @@ def _stats(m, t):
     return float(np.max(np.abs(d) / t)), float(m.min()), float(np.dot(d, d))
 
 
-def solve(diagram, target, w0, tol=1e-10, max_iter=150, rule="damped", ball_cut=False):
+def solve(diagram, target, w0, tol=1e-10, max_iter=150, rule="damped", ball_cut=False, trace=None):
     """diagram: an oracle power diagram (set_weights / der_integrals_wrt_weights);
-    w0: starting weights.  Returns (weights, report)."""
+    w0: starting weights.  Returns (weights, report).  trace (a list, may be
+    None) receives the relative mass error at the start of each iteration."""
     t = np.asarray(target, dtype=np.float64)
     n = t.shape[0]
     w = np.array(w0, dtype=np.float64)
@@ -49,6 +50,8 @@ def solve(diagram, target, w0, tol=1e-10, max_iter=150, rule="damped", ball_cut=
     rep = {"iterations": 0, "evaluations": 1}
     for it in range(max_iter + 1):
         rep["max_rel_mass_error"], rep["min_mass"] = e[0], e[1]
+        if trace is not None:
+            trace.append(e[0])
         if e[0] <= tol:
             rep["converged"] = True
             return w, rep

@@ -115,6 +115,7 @@ SIGNATURES = {
     "sdot_kernel_launches": (ctypes.c_int, [_P]),
     "sdot_measure_fma_peaks": (ctypes.c_int, [_P]),
     "sdot_debug_checks": (ctypes.c_int, [_P]),
+    "sdot_debug_work_counts": (ctypes.c_int, [_P, ctypes.c_int]),
 }
 
 _lib = None

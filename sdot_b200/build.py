@@ -41,14 +41,17 @@ def _compile(src, obj, extra):
     return cmd, r
 
 
-def build(force=False, verbose=False, extra=()):
+def build(force=False, verbose=False, extra=(), lib=None):
     """Compiles every source to an object file (in parallel, one nvcc per
-    file), then links the shared library."""
-    if not force and not needs_rebuild():
+    file), then links the shared library.  lib/extra: another output (e.g.
+    the counting build, -DSDOT_COUNT) with extra compiler flags; its objects
+    go to a folder of their own."""
+    lib = lib or LIB
+    if lib == LIB and not force and not needs_rebuild():
         return LIB
     from concurrent.futures import ThreadPoolExecutor
 
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build" if lib == LIB else "_build_" + os.path.basename(lib).split(".")[0])
     os.makedirs(objdir, exist_ok=True)
     jobs = [(os.path.join(CSRC, s), os.path.join(objdir, s.replace(".cu", ".o"))) for s in SOURCES]
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
@@ -64,13 +67,24 @@ def build(force=False, verbose=False, extra=()):
             sys.stderr.write(r.stdout + r.stderr)
     if failed:
         raise RuntimeError("nvcc failed building libsdot_b200.so")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *[o for _, o in jobs]]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", lib + ".tmp", *[o for _, o in jobs]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed linking libsdot_b200.so")
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+        raise RuntimeError("nvcc failed linking " + os.path.basename(lib))
+    os.replace(lib + ".tmp", lib)
+    return lib
+
+
+COUNT_LIB = os.path.join(HERE, "libsdot_b200_count.so")
+
+
+def build_counting(force=False):
+    """The counting build (-DSDOT_COUNT): the same library with the work
+    counters of the 2D fast tier compiled in (sdot_debug_work_counts)."""
+    if not force and os.path.exists(COUNT_LIB) and os.path.getmtime(COUNT_LIB) >= os.path.getmtime(LIB):
+        return COUNT_LIB
+    return build(force=True, extra=["-DSDOT_COUNT"], lib=COUNT_LIB)
 
 
 if __name__ == "__main__":

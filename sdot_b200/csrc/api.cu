@@ -1482,6 +1482,18 @@ int sdot_debug_checks(uint64_t *out6) {
     return SDOT_OK;
 }
 
+int sdot_debug_work_counts(uint64_t *out8, int reset) {
+    if (!out8) return SDOT_BAD_ARG;
+    unsigned long long a[8];
+    try {
+        cells2d_read_work(a, reset != 0);
+    } catch (const CudaError &) {
+        return SDOT_CUDA_ERROR;
+    }
+    for (int k = 0; k < 8; ++k) out8[k] = a[k];
+    return SDOT_OK;
+}
+
 int sdot_kernel_launches(uint64_t *count) {
     if (!count) return SDOT_BAD_ARG;
     *count = g_launches.load();

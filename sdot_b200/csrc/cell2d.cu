@@ -31,6 +31,18 @@
 
 namespace sdot {
 
+// Counting builds (-DSDOT_COUNT) add up the work of the fast tier's walks,
+// the terms of the per-cell operation count: [0] cut attempts, [1] vertices
+// classified at them, [2] node tests, [3] vertices tested at them, [4]
+// effective cuts, [5] final vertices, [6] cells built.  Release builds
+// compile the counting away.
+#ifdef SDOT_COUNT
+static __device__ unsigned long long sdot_work[8];
+#define SDOT_WORK_ADD(k, v) atomicAdd(&sdot_work[k], (unsigned long long)(v))
+#else
+#define SDOT_WORK_ADD(k, v) ((void)0)
+#endif
+
 namespace {
 
 constexpr int T2D_MAX = 128;  // largest block of the fast kernels (their block size is tuned, see launch_all)
@@ -459,8 +471,11 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             mask |= unsigned(is_cut ? d < 0.0 : !(lhs <= rhs)) << k;
         }
         const CutFacts f = cut_facts(mask, n);
+        SDOT_WORK_ADD(is_cut ? 0 : 2, 1);
+        SDOT_WORK_ADD(is_cut ? 1 : 3, n);
         if (is_cut) {
             if (f.nb_out) {
+                SDOT_WORK_ADD(4, 1);
                 n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, PER ? j + (sym + 1) * int(A.n) : j, true, f);
                 if (n <= 0) return n;
             }
@@ -979,6 +994,8 @@ __global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d(const Cell2DArgs A) {
     const long long s = blockIdx.x * (long long)T2D + t;
     if (s >= A.n) return;
     const int n = build_cell<MODE == DM_PERIODIC>(A, s, cell, CAP, A.pos[2 * s], A.pos[2 * s + 1], A.w[s]);
+    SDOT_WORK_ADD(5, n > 0 ? n : 0);
+    SDOT_WORK_ADD(6, 1);
     Out row(A.rows.cnt ? A.rows.col + s : nullptr, A.rows.cnt ? A.rows.val + s : nullptr, A.rows.stride, A.rows.cap);
     Out nbo(A.nb.cnt ? A.nb.col + s : nullptr, nullptr, A.nb.stride, A.nb.cap);
     if (finish_cell<MODE, BALL>(A, s, cell, n, acc, T2D, row, nbo)) {
@@ -1320,6 +1337,19 @@ void cells2d_read_checks(unsigned long long out[3]) {
     SDOT_CUDA(cudaMemcpyFromSymbol(out, sdot_dbg_word, 3 * sizeof(unsigned long long)));
 #else
     out[0] = out[1] = out[2] = 0;
+#endif
+}
+
+void cells2d_read_work(unsigned long long out[8], bool reset) {
+#ifdef SDOT_COUNT
+    SDOT_CUDA(cudaMemcpyFromSymbol(out, sdot_work, 8 * sizeof(unsigned long long)));
+    if (reset) {
+        const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        SDOT_CUDA(cudaMemcpyToSymbol(sdot_work, z, sizeof z));
+    }
+#else
+    (void)reset;
+    for (int k = 0; k < 8; ++k) out[k] = 0;
 #endif
 }
 

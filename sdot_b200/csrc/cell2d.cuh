@@ -105,6 +105,9 @@ size_t cells2d_scratch_bytes();
 // First failed debug check of the cell kernels (code, line, value); zeros in
 // release builds.
 void cells2d_read_checks(unsigned long long out[3]);
+// Work counts of the fast tier's walks (counting builds, -DSDOT_COUNT; zeros
+// otherwise), optionally reset.
+void cells2d_read_work(unsigned long long out[8], bool reset);
 // Fast kernel over all cells, then the big and huge tiers over the overflow
 // lists.  `scratch` must hold cells2d_scratch_bytes() bytes.
 void cells2d_launch(const Cell2DArgs &a, void *scratch, cudaStream_t st);

@@ -136,7 +136,11 @@ def test_image_poly6(gpu_lib, ref_oracle, n, res):
     img = rng.uniform(-0.3, 0.3, (6,) + res)
     img[0] += 2.0
     gpu, ref = make_pair(p, w, ref_oracle, image=img)
-    check_all(gpu, ref, n)
+    # the boundary measures: Simpson along each edge here, the reference's
+    # expanded closed form in absolute coordinates there; on the short edges
+    # of the 100k case the C restatement (also Simpson) and the reference
+    # already differ by 3.0e-12 of the mean diagonal: Hessian bound 1e-11
+    check_all(gpu, ref, n, rtol_hess=1e-11)
     assert abs(gpu.domain_measure() - ref.domain_measure()) <= 1e-13 * ref.domain_measure()
 
 

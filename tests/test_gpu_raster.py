@@ -9,8 +9,8 @@ pixel value of that component).
 Cell numbers: where several cells meet a pixel the reference keeps the one
 its work order wrote last and the GPU the largest index; both must mark the
 same pixels as covered, the GPU's index is never below the reference's (the
-reference's is one of the covering cells), and they agree on the pixels that
-lie inside one cell.
+reference's is one of the covering cells), and where they differ the GPU's
+cell borders the reference's one.
 """
 import numpy as np
 import pytest
@@ -66,10 +66,11 @@ def test_image_of_cell_nums(gpu_lib, ref_oracle):
     r = ref.image_of_cell_nums([0.0, 0.0], [1.0, 1.0], nbp)
     assert ((g < 0) == (r < 0)).all()
     assert (g >= r).all()
-    # pixels whose four neighbours carry the same reference number lie inside
-    # one cell (cells span ~9 pixels): there the numbers must agree
-    inner = np.zeros_like(r, dtype=bool)
-    inner[1:-1, 1:-1] = ((r[1:-1, 1:-1] == r[:-2, 1:-1]) & (r[1:-1, 1:-1] == r[2:, 1:-1]) &
-                         (r[1:-1, 1:-1] == r[1:-1, :-2]) & (r[1:-1, 1:-1] == r[1:-1, 2:]))
-    assert inner.sum() > 0.3 * inner.size
-    assert (g[inner] == r[inner]).mean() > 0.99
+    # where they differ, the pixel meets two cells (pixels are ~1/100 of a
+    # cell): the GPU's cell is then a neighbour of the reference's one
+    off, ids = ref.neighbors()
+    diff = np.argwhere(g != r)
+    assert len(diff) < 0.2 * g.size
+    for iy, ix in diff:
+        a, b = int(r[iy, ix]), int(g[iy, ix])
+        assert b in set(ids[off[a]:off[a + 1]].tolist()), (iy, ix, a, b)
