@@ -488,7 +488,11 @@ def newton_leg():
           tests/golden/newton_floor_c2.json), so the clamped mix runs to 1e-3
           and the same mix with the clustered Diracs mirrored at the faces
           (closest pairs ~3e-7 apart) to 1e-7;
-      C3  500k, 512^2 image, disc clip, w0 = (0.5/sqrt n)^2, targets 0.8/n, to 1e-8;
+      C3  500k, 512^2 image, disc clip, w0 = (0.5/sqrt n)^2, targets 0.8/n, to 1e-8,
+          at most 30 iterations: from this start the damped Newton (and the
+          reference's own rule) advances slowly -- the Newton oracle over the
+          compiled reference is still at a relative mass error of 0.2 after 60
+          iterations at 20k Diracs -- so the leg reports the error reached;
       C4  200k 3D mix, density (1 + 0.3 xyz) normalised, w = 0, to 1e-8."""
     from sdot_b200 import workloads
     from sdot_b200.power_diagram import PowerDiagram
@@ -504,7 +508,7 @@ def newton_leg():
              ("C2_1M_clamped_from_w0_to_1e-3", c2["positions"], None, 1e-3, {}),
              ("C2_1M_mirrored_from_w0_to_1e-7", mirrored, None, 1e-7, {}),
              ("C3_500k_image_disc_to_1e-8", c3["positions"], c3["weights"], 1e-8,
-              {"image": c3["image"], "target": c3["target"], "radial_func": "in_ball_w05"}),
+              {"image": c3["image"], "target": c3["target"], "radial_func": "in_ball_w05", "max_iter": 30}),
              ("C4_200k_3d_to_1e-8", c4["positions"], None, 1e-8, {"density": c4["density"]})]
     out = {}
     for name, pos, w0, tol, extra in cases:
@@ -523,14 +527,15 @@ def newton_leg():
             key = f"{name}_{ls}"
             t0 = time.perf_counter()
             try:
-                rep = g.solve_weights(t, rel_mass_tol=tol, linear_solver=ls)
+                rep = g.solve_weights(t, rel_mass_tol=tol, linear_solver=ls, max_iter=extra.get("max_iter", 150),
+                                      raise_on_failure=False)
             except Exception as e:
                 out[key] = {"error": str(e), "time_s": time.perf_counter() - t0}
                 continue
             wall = time.perf_counter() - t0
-            out[key] = {"time_s": wall, "iterations": rep["iterations"], "pcg_iterations": int(rep["pcg_iterations"]),
-                        "pcg_levels": rep["pcg_levels"], "evaluations": rep["evaluations"],
-                        "max_rel_mass_error": rep["max_rel_mass_error"]}
+            out[key] = {"time_s": wall, "converged": rep["status"] == 0, "iterations": rep["iterations"],
+                        "pcg_iterations": int(rep["pcg_iterations"]), "pcg_levels": rep["pcg_levels"],
+                        "evaluations": rep["evaluations"], "max_rel_mass_error": rep["max_rel_mass_error"]}
     return out
 
 

@@ -90,16 +90,19 @@ class Cell:
         self.centre = centre
 
 
-def build_cell(i, pos, w, lo, hi, cand=None):
-    """Power cell of Dirac i in the box [lo, hi] (None when empty)."""
+def build_cell(i, pos, w, lo, hi, cand=None, planes=None):
+    """Power cell of Dirac i in the box [lo, hi] cut by the half-spaces
+    planes[k, :3] . x <= planes[k, 3] (ids -7 - k; None: the box alone),
+    None when empty."""
     n = len(pos)
     js = np.arange(n) if cand is None else np.asarray(cand)
     js = js[js != i]
     V = pos[js] - pos[i]
-    A = np.vstack([V, -np.eye(3), np.eye(3)])
+    P4 = np.zeros((0, 4)) if planes is None else np.asarray(planes, float).reshape(-1, 4)
+    A = np.vstack([V, -np.eye(3), np.eye(3), P4[:, :3]])
     b = np.concatenate([0.5 * (np.sum(pos[js] ** 2, 1) - np.sum(pos[i] ** 2) + w[i] - w[js]),
-                        -np.asarray(lo, float), np.asarray(hi, float)])
-    ids = np.concatenate([js, -1 - np.arange(6)])
+                        -np.asarray(lo, float), np.asarray(hi, float), P4[:, 3]])
+    ids = np.concatenate([js, -1 - np.arange(6), -7 - np.arange(len(P4))])
     x0 = _chebyshev_centre(A, b)
     if x0 is None:
         return None
@@ -117,7 +120,7 @@ def build_cell(i, pos, w, lo, hi, cand=None):
     return Cell(tris, ids[h], x0)
 
 
-def cells(pos, w=None, lo=(0, 0, 0), hi=(1, 1, 1)):
+def cells(pos, w=None, lo=(0, 0, 0), hi=(1, 1, 1), planes=None):
     """All cells; candidates grow from nearest neighbours until no other Dirac
     can cut (its bisector is farther than the cell's farthest vertex)."""
     pos = np.asarray(pos, float)
@@ -129,7 +132,7 @@ def cells(pos, w=None, lo=(0, 0, 0), hi=(1, 1, 1)):
         near = np.argsort(d2)
         k = min(n, 48)
         while True:
-            c = build_cell(i, pos, w, lo, hi, near[:k])
+            c = build_cell(i, pos, w, lo, hi, near[:k], planes)
             if c is None or k == n:
                 break
             r = np.max(np.linalg.norm(c.tris.reshape(-1, 3) - pos[i], axis=1))
@@ -144,14 +147,15 @@ def cells(pos, w=None, lo=(0, 0, 0), hi=(1, 1, 1)):
     return out
 
 
-def integrate(pos, w=None, poly=None, coeff=1.0, lo=(0, 0, 0), hi=(1, 1, 1)):
+def integrate(pos, w=None, poly=None, coeff=1.0, lo=(0, 0, 0), hi=(1, 1, 1), planes=None):
     """Masses (n), centroids (n, 3) and the Hessian as {(i, j): value} for
-    density coeff * sum_m poly[m] * MONOMIALS[m] (poly None: constant)."""
+    density coeff * sum_m poly[m] * MONOMIALS[m] (poly None: constant) over
+    the box [lo, hi] cut by `planes` (see build_cell)."""
     pos = np.asarray(pos, float)
     n = len(pos)
     w = np.zeros(n) if w is None else np.asarray(w, float)
     poly = np.array([1.0, 0, 0, 0, 0, 0, 0, 0]) if poly is None else np.asarray(poly, float)
-    cs = cells(pos, w, lo, hi)
+    cs = cells(pos, w, lo, hi, planes)
     mass = np.zeros(n)
     ctd = np.zeros((n, 3))
     H = {}
@@ -198,3 +202,23 @@ def box_integral(poly, lo=(0, 0, 0), hi=(1, 1, 1)):
             t *= 0.5 * (hi[d] ** 2 - lo[d] ** 2) if d in cl else hi[d] - lo[d]
         res += t
     return res
+
+
+def integrate_shapes(pos, shapes, w=None, poly=None):
+    """A domain of several convex shapes (ConvexPolyhedronAssembly: each
+    cell is intersected with every shape and the pieces summed,
+    ConvexPolyhedronAssembly.tcc:132-142).  shapes: list of (lo, hi, planes,
+    coeff).  Returns masses, centroids and the Hessian dict like integrate."""
+    pos = np.asarray(pos, float)
+    n = len(pos)
+    mass = np.zeros(n)
+    mom = np.zeros((n, 3))
+    H = {}
+    for lo, hi, planes, coeff in shapes:
+        m, c, h = integrate(pos, w, poly, coeff, lo, hi, planes)
+        mass += m
+        mom += c * m[:, None]
+        for k, v in h.items():
+            H[k] = H.get(k, 0.0) + v
+    ctd = np.where(mass[:, None] != 0, mom / np.where(mass == 0, 1.0, mass)[:, None], 0.0)
+    return mass, ctd, H

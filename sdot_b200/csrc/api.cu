@@ -9,6 +9,7 @@
 #include "tree.cuh"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -89,6 +90,113 @@ Item2 box_item(double x0, double y0, double x1, double y1, double coeff) {
     return it;
 }
 
+// A convex polyhedron on the host, as faces (vertex loops counter-clockwise
+// seen from outside): the domain shapes of 3D contexts, for their measures.
+struct HostPoly3 {
+    using P3 = std::array<double, 3>;
+    std::vector<std::vector<P3>> faces;
+
+    static HostPoly3 box(const double *lo, const double *hi) {
+        HostPoly3 p;
+        auto c = [&](int k) { return P3{(k & 1) ? hi[0] : lo[0], (k & 2) ? hi[1] : lo[1], (k & 4) ? hi[2] : lo[2]}; };
+        const int f[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
+        for (auto &q : f) p.faces.push_back({c(q[0]), c(q[1]), c(q[2]), c(q[3])});
+        return p;
+    }
+    // keeps a . x <= b
+    void cut(const double *a, double b) {
+        auto d = [&](const P3 &v) { return a[0] * v[0] + a[1] * v[1] + a[2] * v[2] - b; };
+        std::vector<std::vector<P3>> out;
+        std::vector<P3> cap;  // points on the plane: the new face
+        for (const auto &f : faces) {
+            std::vector<P3> g;
+            for (size_t i = 0; i < f.size(); ++i) {
+                const P3 &u = f[i], &v = f[(i + 1) % f.size()];
+                const double du = d(u), dv = d(v);
+                if (du <= 0) g.push_back(u);
+                if ((du < 0 && dv > 0) || (du > 0 && dv < 0)) {
+                    const double t = du / (du - dv);
+                    const P3 x{u[0] + t * (v[0] - u[0]), u[1] + t * (v[1] - u[1]), u[2] + t * (v[2] - u[2])};
+                    g.push_back(x);
+                    cap.push_back(x);
+                } else if (du == 0) {
+                    cap.push_back(u);
+                }
+            }
+            if (g.size() >= 3) out.push_back(g);
+        }
+        if (cap.size() >= 3) {
+            // order the new face's points counter-clockwise around a (outward)
+            P3 c{0, 0, 0};
+            for (const P3 &x : cap)
+                for (int k = 0; k < 3; ++k) c[k] += x[k] / double(cap.size());
+            const double na = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+            const P3 nn{a[0] / na, a[1] / na, a[2] / na};
+            P3 e1{cap[0][0] - c[0], cap[0][1] - c[1], cap[0][2] - c[2]};
+            const double l1 = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+            if (l1 > 0) {
+                for (double &x : e1) x /= l1;
+                const P3 e2{nn[1] * e1[2] - nn[2] * e1[1], nn[2] * e1[0] - nn[0] * e1[2], nn[0] * e1[1] - nn[1] * e1[0]};
+                std::vector<std::pair<double, P3>> ang;
+                for (const P3 &x : cap) {
+                    const P3 v{x[0] - c[0], x[1] - c[1], x[2] - c[2]};
+                    ang.push_back({std::atan2(v[0] * e2[0] + v[1] * e2[1] + v[2] * e2[2],
+                                              v[0] * e1[0] + v[1] * e1[1] + v[2] * e1[2]), x});
+                }
+                std::sort(ang.begin(), ang.end(), [](const auto &p, const auto &q) { return p.first < q.first; });
+                std::vector<P3> face;
+                for (const auto &pa : ang)
+                    if (face.empty() || std::abs(pa.second[0] - face.back()[0]) + std::abs(pa.second[1] - face.back()[1]) +
+                                                std::abs(pa.second[2] - face.back()[2]) > 0)
+                        face.push_back(pa.second);
+                if (face.size() >= 3) out.push_back(face);
+            }
+        }
+        faces.swap(out);
+    }
+    // integral of c0 + c1 x + c2 y + c3 z + c4 xy + c5 xz + c6 yz + c7 xyz:
+    // tetrahedra from the vertices' mean to each fan triangle, each by the
+    // degree-3 five-point rule (weight -4/5 at the centroid, 9/20 at the four
+    // points with barycentric coordinates (1/2, 1/6, 1/6, 1/6); P. Keast,
+    // "Moderate-degree tetrahedral quadrature formulas", CMAME 55, 1986),
+    // exact for this density
+    double integrate(const double *c) const {
+        P3 o{0, 0, 0};
+        size_t cnt = 0;
+        for (const auto &f : faces)
+            for (const P3 &x : f) {
+                for (int k = 0; k < 3; ++k) o[k] += x[k];
+                ++cnt;
+            }
+        if (!cnt) return 0;
+        for (double &x : o) x /= double(cnt);
+        auto fv = [&](const P3 &x) {
+            return c[0] + c[1] * x[0] + c[2] * x[1] + c[3] * x[2] + c[4] * x[0] * x[1] + c[5] * x[0] * x[2] +
+                   c[6] * x[1] * x[2] + c[7] * x[0] * x[1] * x[2];
+        };
+        double res = 0;
+        for (const auto &f : faces)
+            for (size_t i = 1; i + 1 < f.size(); ++i) {
+                const P3 v[4] = {o, f[0], f[i], f[i + 1]};
+                const double ux = v[1][0] - o[0], uy = v[1][1] - o[1], uz = v[1][2] - o[2];
+                const double vx = v[2][0] - o[0], vy = v[2][1] - o[1], vz = v[2][2] - o[2];
+                const double wx = v[3][0] - o[0], wy = v[3][1] - o[1], wz = v[3][2] - o[2];
+                const double vol = (ux * (vy * wz - vz * wy) - uy * (vx * wz - vz * wx) + uz * (vx * wy - vy * wx)) / 6;
+                P3 g{0, 0, 0};
+                for (int k = 0; k < 4; ++k)
+                    for (int d = 0; d < 3; ++d) g[d] += 0.25 * v[k][d];
+                double q = -0.8 * fv(g);
+                for (int k = 0; k < 4; ++k) {
+                    P3 x;
+                    for (int d = 0; d < 3; ++d) x[d] = 0.5 * v[k][d] + (1.0 / 6.0) * (v[0][d] + v[1][d] + v[2][d] + v[3][d] - v[k][d]);
+                    q += 0.45 * fv(x);
+                }
+                res += vol * q;
+            }
+        return res;
+    }
+};
+
 }  // namespace
 
 struct sdot_ctx {
@@ -109,10 +217,16 @@ struct sdot_ctx {
 
     // domain (host side)
     std::vector<Item2> items;
-    struct Box3 {
+    // a 3D domain shape: its box, cut by the half-spaces a . x <= b (4
+    // doubles per plane; none for a box), and its density
+    struct Item3 {
         double lo[3], hi[3], coeff;
+        std::vector<double> planes;
     };
-    std::vector<Box3> boxes3;  // 3D domain: boxes (one supported)
+    std::vector<Item3> items3;
+    double *d_planes3 = nullptr;       // every shape's planes, shape k from plane_off3[k]
+    std::vector<int> plane_off3;
+    bool planes3_dirty = true;
     bool has_poly = false;     // 3D multilinear density factor
     double poly3[8] = {1, 0, 0, 0, 0, 0, 0, 0};
     bool has_image = false;
@@ -186,6 +300,7 @@ struct sdot_ctx {
         dfree(d_pos); dfree(d_w);
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
         dfree(d_trans);
+        dfree(d_planes3);
         free_eval();
         free_newton();
         free_multi();
@@ -366,11 +481,21 @@ struct sdot_ctx {
     // the domain is one the kernels handle; uploads the 2D one
     void check_domain() {
         if (dim == 3) {
-            if (boxes3.size() != 1)
-                throw Unsupported(boxes3.empty() ? "no domain: call sdot_add_box_shape first"
-                                                 : "3D domains of several boxes are not available in this build");
+            if (items3.empty()) throw BadArg("no domain: call sdot_add_box_shape (or another add_..._shape) first");
             if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
             if (!trans_h.empty()) throw Unsupported("periodic translations are available in 2D only");
+            if (planes3_dirty) {
+                std::vector<double> all;
+                plane_off3.assign(1, 0);
+                for (const Item3 &it : items3) {
+                    all.insert(all.end(), it.planes.begin(), it.planes.end());
+                    plane_off3.push_back(int(all.size() / 4));
+                }
+                dalloc(d_planes3, all.size());
+                if (!all.empty())
+                    SDOT_CUDA(cudaMemcpy(d_planes3, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+                planes3_dirty = false;
+            }
             return;
         }
         if (!trans_h.empty() && (long long)(trans_h.size() / 2 + 1) * n >= (1LL << 31))
@@ -387,8 +512,8 @@ struct sdot_ctx {
         if (mcap >= n && t_mass) return;
         free_multi();
         mcap = std::max<long long>(n, 1);
-        alloc_rows(rows_tmp, mcap, ROWCAP_2D, true);
-        dalloc(t_mass, mcap); dalloc(t_mass_c, mcap); dalloc(t_ctd, 2 * mcap); dalloc(s_mom, 2 * mcap);
+        alloc_rows(rows_tmp, mcap, dim == 3 ? ROWCAP_3D : ROWCAP_2D, true);
+        dalloc(t_mass, mcap); dalloc(t_mass_c, mcap); dalloc(t_ctd, size_t(dim) * mcap); dalloc(s_mom, size_t(dim) * mcap);
     }
     void free_multi() {
         free_rows(rows_tmp);
@@ -420,24 +545,68 @@ struct sdot_ctx {
             a.ctd = t_ctd;
             a.rows = rows_tmp;
             cells2d_launch(a, scratch, stream);
-            accum_pass2(s_mass, s_mass_c, s_mom, t_mass, t_mass_c, t_ctd, n, stream);
+            accum_pass(s_mass, s_mass_c, s_mom, t_mass, t_mass_c, t_ctd, n, 2, stream);
             rows_append(rows, rows_tmp, n, err, stream);
         }
-        centroids_final2(s_ctd, s_mom, s_mass_c, n, stream);
+        centroids_final(s_ctd, s_mom, s_mass_c, n, 2, stream);
     }
 
-    Cell3DArgs args3() {
+    // The 3D counterpart: one pass per shape (the shape's box cut by its
+    // planes as the starting polyhedron), summed.  The cells' pass hints
+    // belong to one starting polyhedron, so these passes neither use nor
+    // record them.
+    void evaluate_multi3() {
+        reserve_multi();
+        SDOT_CUDA(cudaMemsetAsync(s_mass, 0, size_t(n) * sizeof(double), stream));
+        SDOT_CUDA(cudaMemsetAsync(s_mass_c, 0, size_t(n) * sizeof(double), stream));
+        SDOT_CUDA(cudaMemsetAsync(s_mom, 0, size_t(3 * n) * sizeof(double), stream));
+        rows_clear(rows, n, stream);
+        SDOT_CUDA(cudaMemsetAsync(rows.side_used, 0, sizeof(unsigned long long), stream));
+        for (size_t k = 0; k < items3.size(); ++k) {
+            Cell3DArgs a = args3(int(k));
+            a.hint = nullptr;
+            a.use_hint = 0;
+            a.mass = t_mass;
+            a.ctd = t_ctd;
+            a.rows = rows_tmp;
+            cells3d_launch(a, scratch3, stream);
+            accum_pass(s_mass, s_mass_c, s_mom, t_mass, t_mass, t_ctd, n, 3, stream);
+            rows_append(rows, rows_tmp, n, err, stream);
+        }
+        centroids_final(s_ctd, s_mom, s_mass_c, n, 3, stream);
+        hint_valid = false;
+    }
+
+    // arguments of a pass over shape k of the 3D domain (k = -1: the box
+    // englobing every shape, inflated by its size as
+    // ConvexPolyhedronAssembly::englobing_convex_polyhedron makes it, density 1)
+    Cell3DArgs args3(int k = 0) {
         Cell3DArgs a;
         a.n = n;
         a.pos = tree3.pos;
         a.w = tree3.w;
         a.nodes = tree3.nodes;
         a.max_nodes = tree3.max_nodes;
-        for (int d = 0; d < 3; ++d) {
-            a.box_lo[d] = boxes3[0].lo[d];
-            a.box_hi[d] = boxes3[0].hi[d];
+        if (k >= 0) {
+            for (int d = 0; d < 3; ++d) {
+                a.box_lo[d] = items3[k].lo[d];
+                a.box_hi[d] = items3[k].hi[d];
+            }
+            a.coeff = items3[k].coeff;
+            a.nplanes = plane_off3[k + 1] - plane_off3[k];
+            a.planes = a.nplanes ? d_planes3 + 4 * plane_off3[k] : nullptr;
+        } else {
+            for (int d = 0; d < 3; ++d) {
+                double lo = items3[0].lo[d], hi = items3[0].hi[d];
+                for (const Item3 &it : items3) {
+                    lo = std::min(lo, it.lo[d]);
+                    hi = std::max(hi, it.hi[d]);
+                }
+                a.box_lo[d] = lo - (hi - lo);
+                a.box_hi[d] = hi + (hi - lo);
+            }
+            a.coeff = 1.0;
         }
-        a.coeff = boxes3[0].coeff;
         a.has_poly = has_poly ? 1 : 0;
         for (int k = 0; k < 8; ++k) a.poly[k] = poly3[k];
         a.ovf_list = ovf_list;
@@ -483,8 +652,10 @@ struct sdot_ctx {
         SDOT_CUDA(cudaEventRecord(ev[0], stream));
         ensure_tree();
         SDOT_CUDA(cudaEventRecord(ev[1], stream));
-        if (dim == 3) {
-            Cell3DArgs a = args3();
+        if (dim == 3 && items3.size() > 1) {
+            evaluate_multi3();
+        } else if (dim == 3) {
+            Cell3DArgs a = args3(0);
             a.mass = s_mass;
             a.ctd = s_ctd;
             a.rows = rows;
@@ -528,7 +699,7 @@ struct sdot_ctx {
             // (not when the evaluation failed anyway)
             ++side_retries;
             grow_side(rows);
-            if (dim != 3 && mode == DM_MULTI) grow_side(rows_tmp);
+            if ((dim != 3 && mode == DM_MULTI) || (dim == 3 && items3.size() > 1)) grow_side(rows_tmp);
             const int st = evaluate();
             side_retries = 0;
             return st;
@@ -584,7 +755,12 @@ struct sdot_ctx {
         for (int attempt = 0;; ++attempt) {
             SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
             if (dim == 3) {
-                Cell3DArgs a = args3();
+                // several shapes: the traversal cell in the englobing box
+                Cell3DArgs a = args3(items3.size() > 1 ? -1 : 0);
+                if (items3.size() > 1) {
+                    a.hint = nullptr;
+                    a.use_hint = 0;
+                }
                 a.nb = nb;
                 cells3d_launch(a, scratch3, stream);
             } else {
@@ -1004,8 +1180,9 @@ int sdot_add_box_shape(sdot_ctx *ctx, const double *p0, const double *p1, double
         if (!p0 || !p1) throw BadArg("null box corner");
         ctx->has_image = false;
         if (ctx->dim == 3) {
-            sdot_ctx::Box3 b{{p0[0], p0[1], p0[2]}, {p1[0], p1[1], p1[2]}, coeff};
-            ctx->boxes3.push_back(b);
+            sdot_ctx::Item3 b{{p0[0], p0[1], p0[2]}, {p1[0], p1[1], p1[2]}, coeff, {}};
+            ctx->items3.push_back(b);
+            ctx->planes3_dirty = true;
         } else {
             ctx->items.push_back(box_item(p0[0], p0[1], p1[0], p1[1], coeff));
         }
@@ -1019,7 +1196,35 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
                                      double coeff) {
     return guarded(ctx, [&] {
         if (m <= 0 || !points || !normals) throw BadArg("bad convex polyhedron");
-        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
+        if (ctx->dim == 3) {
+            // ConvexPolyhedronAssembly::add_convex_polyhedron (.tcc:7-33): the
+            // bounding box of the points inflated by its size on each side,
+            // cut by each (point, normalized normal) half-space
+            sdot_ctx::Item3 it;
+            it.coeff = coeff;
+            for (int d = 0; d < 3; ++d) {
+                double mn = std::numeric_limits<double>::max(), mx = -std::numeric_limits<double>::max();
+                for (int64_t i = 0; i < m; ++i) {
+                    mn = std::min(mn, points[3 * i + d]);
+                    mx = std::max(mx, points[3 * i + d]);
+                }
+                it.lo[d] = mn - (mx - mn);
+                it.hi[d] = mx + (mx - mn);
+            }
+            for (int64_t i = 0; i < m; ++i) {
+                const double *q = normals + 3 * i, *p = points + 3 * i;
+                const double l = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) + 1e-40;  // Point3 normalized()
+                const double a[3] = {q[0] / l, q[1] / l, q[2] / l};
+                it.planes.insert(it.planes.end(), {a[0], a[1], a[2], a[0] * p[0] + a[1] * p[1] + a[2] * p[2]});
+            }
+            if (it.planes.size() / 4 > 64) throw Unsupported("a 3D shape has more than 64 faces");
+            ctx->has_image = false;
+            ctx->items3.push_back(std::move(it));
+            ctx->planes3_dirty = true;
+            ctx->dom_dirty = true;
+            ctx->mark_dirty();
+            return int(SDOT_OK);
+        }
         // ConvexPolyhedronAssembly::add_convex_polyhedron: the bounding box of
         // the points inflated by its size, cut by each (point, normal) half-plane.
         double mn[2], mx[2];
@@ -1078,7 +1283,34 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
 int sdot_add_simplex_shape(sdot_ctx *ctx, const double *pts, double coeff) {
     return guarded(ctx, [&] {
         if (!pts) throw BadArg("null simplex");
-        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
+        if (ctx->dim == 3) {
+            // a tetrahedron: its bounding box cut by its four face planes, each
+            // oriented away from the opposite vertex
+            sdot_ctx::Item3 it;
+            it.coeff = coeff;
+            for (int d = 0; d < 3; ++d) {
+                it.lo[d] = std::min(std::min(pts[d], pts[3 + d]), std::min(pts[6 + d], pts[9 + d]));
+                it.hi[d] = std::max(std::max(pts[d], pts[3 + d]), std::max(pts[6 + d], pts[9 + d]));
+            }
+            const int face[4][4] = {{1, 2, 3, 0}, {0, 2, 3, 1}, {0, 1, 3, 2}, {0, 1, 2, 3}};  // 3 vertices, opposite
+            for (const auto &f : face) {
+                const double *a = pts + 3 * f[0], *b = pts + 3 * f[1], *c = pts + 3 * f[2], *o = pts + 3 * f[3];
+                const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, v[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+                double nrm[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+                const double l = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+                if (!(l > 0)) throw BadArg("degenerate simplex");
+                double side = nrm[0] * (o[0] - a[0]) + nrm[1] * (o[1] - a[1]) + nrm[2] * (o[2] - a[2]);
+                const double sg = side > 0 ? -1.0 : 1.0;
+                for (double &x : nrm) x *= sg / l;
+                it.planes.insert(it.planes.end(), {nrm[0], nrm[1], nrm[2], nrm[0] * a[0] + nrm[1] * a[1] + nrm[2] * a[2]});
+            }
+            ctx->has_image = false;
+            ctx->items3.push_back(std::move(it));
+            ctx->planes3_dirty = true;
+            ctx->dom_dirty = true;
+            ctx->mark_dirty();
+            return int(SDOT_OK);
+        }
         // ConvexPolyhedron2( Simplex ) (ConvexPolyhedron2.tcc:19-60)
         double p[3][2] = {{pts[0], pts[1]}, {pts[2], pts[3]}, {pts[4], pts[5]}};
         double cx = 1.0 / 3 * (p[0][0] + p[1][0] + p[2][0]), cy = 1.0 / 3 * (p[0][1] + p[1][1] + p[2][1]);
@@ -1151,7 +1383,8 @@ int sdot_set_polynomial_density(sdot_ctx *ctx, const double *coeffs, int nb_coef
 int sdot_clear_domain(sdot_ctx *ctx) {
     return guarded(ctx, [&] {
         ctx->items.clear();
-        ctx->boxes3.clear();
+        ctx->items3.clear();
+        ctx->planes3_dirty = true;
         ctx->has_poly = false;
         for (int k = 0; k < 8; ++k) ctx->poly3[k] = k == 0 ? 1.0 : 0.0;
         ctx->has_image = false;
@@ -1191,16 +1424,24 @@ static double domain_measure(const sdot_ctx *ctx) {
     }
     double res = 0;
     for (const Item2 &it : ctx->items) res += it.coeff * it.area();
-    for (const sdot_ctx::Box3 &b : ctx->boxes3) {
-        // integral over the box of the multilinear factor: per monomial, a
-        // product over the axes of (hi - lo) or (hi^2 - lo^2) / 2
-        static const int axes[8] = {0, 1, 2, 4, 3, 5, 6, 7};  // bit d: u_d in the monomial
+    for (const sdot_ctx::Item3 &b : ctx->items3) {
         double f = 0;
-        for (int k = 0; k < 8; ++k) {
-            double t = ctx->poly3[k];
-            for (int d = 0; d < 3; ++d)
-                t *= (axes[k] >> d & 1) ? 0.5 * (b.hi[d] * b.hi[d] - b.lo[d] * b.lo[d]) : b.hi[d] - b.lo[d];
-            f += t;
+        if (b.planes.empty()) {
+            // integral over the box of the multilinear factor: per monomial, a
+            // product over the axes of (hi - lo) or (hi^2 - lo^2) / 2
+            static const int axes[8] = {0, 1, 2, 4, 3, 5, 6, 7};  // bit d: u_d in the monomial
+            for (int k = 0; k < 8; ++k) {
+                double t = ctx->poly3[k];
+                for (int d = 0; d < 3; ++d)
+                    t *= (axes[k] >> d & 1) ? 0.5 * (b.hi[d] * b.hi[d] - b.lo[d] * b.lo[d]) : b.hi[d] - b.lo[d];
+                f += t;
+            }
+        } else {
+            // the shape's polyhedron built on the host and integrated
+            // (ConvexPolyhedron3::measure with the multilinear factor)
+            HostPoly3 hp = HostPoly3::box(b.lo, b.hi);
+            for (size_t k = 0; k + 3 < b.planes.size(); k += 4) hp.cut(&b.planes[k], b.planes[k + 3]);
+            f = hp.integrate(ctx->poly3);
         }
         res += b.coeff * f;
     }
@@ -1215,7 +1456,7 @@ int sdot_normalize_domain(sdot_ctx *ctx) {
                 for (double &v : ctx->img_data) v /= mea;
             else {
                 for (Item2 &it : ctx->items) it.coeff /= mea;
-                for (sdot_ctx::Box3 &b : ctx->boxes3) b.coeff /= mea;
+                for (sdot_ctx::Item3 &b : ctx->items3) b.coeff /= mea;
             }
         }
         ctx->dom_dirty = true;

@@ -387,6 +387,15 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
     const double c0x = A.pos[3 * s], c0y = A.pos[3 * s + 1], c0z = A.pos[3 * s + 2], w0 = A.w[s];
     init_box(C, A, c0x, c0y, c0z);
     int status = 0;
+    // a convex shape: its half-spaces cut the box first (relative to c0:
+    // a . u <= b - a . c0), as ConvexPolyhedronAssembly::add_convex_polyhedron
+    // cuts its box (ConvexPolyhedronAssembly.tcc:7-33)
+    for (int k = 0; k < A.nplanes && status == 0; ++k) {
+        const double ax = A.planes[4 * k], ay = A.planes[4 * k + 1], az = A.planes[4 * k + 2];
+        const double b = A.planes[4 * k + 3] - (ax * c0x + ay * c0y + az * c0z);
+        const int r = cut3(C, ax, ay, az, b, domain_id(6 + k));
+        if (r) status = r;
+    }
     if (lane == 0) C.stack[0] = 0;
     __syncwarp();
     int sp = 1;

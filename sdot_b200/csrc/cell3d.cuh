@@ -18,8 +18,13 @@ struct Cell3DArgs {
     const double *w = nullptr;    // n, sorted order
     const TreeNode<3> *nodes = nullptr;
     int max_nodes = 1 << 30;
-    double box_lo[3] = {0, 0, 0}, box_hi[3] = {1, 1, 1};  // the domain (one box)
-    double coeff = 1.0;                                    // its density
+    double box_lo[3] = {0, 0, 0}, box_hi[3] = {1, 1, 1};  // the starting box (a domain shape's box)
+    double coeff = 1.0;                                    // the shape's density
+    // a convex shape: the box cut by nplanes half-spaces a . x <= b
+    // (absolute coordinates; 4 doubles per plane: a, b); faces of the shape
+    // get the ids domain_id(6 + k)
+    int nplanes = 0;
+    const double *planes = nullptr;
     // optional multilinear density factor (has_poly): coeff * (p0 + p1 x +
     // p2 y + p3 z + p4 xy + p5 xz + p6 yz + p7 xyz), absolute coordinates
     int has_poly = 0;

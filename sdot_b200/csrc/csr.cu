@@ -154,24 +154,22 @@ __global__ void k_rows_append(Rows dst, Rows src, long long n, unsigned *err) {
     dst.cnt[s] = m;
 }
 
-// mass += t_mass, mass_c += t_mass_c, mom += t_ctd * t_mass_c (2D)
-__global__ void k_accum2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
-                         const double *t_ctd, long long n) {
+// mass += t_mass, mass_c += t_mass_c, mom += t_ctd * t_mass_c (dim 2 or 3)
+__global__ void k_accum(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                        const double *t_ctd, long long n, int dim) {
     const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= n) return;
     mass[s] += t_mass[s];
     mass_c[s] += t_mass_c[s];
-    mom[2 * s] += t_ctd[2 * s] * t_mass_c[s];
-    mom[2 * s + 1] += t_ctd[2 * s + 1] * t_mass_c[s];
+    for (int d = 0; d < dim; ++d) mom[dim * s + d] += t_ctd[dim * s + d] * t_mass_c[s];
 }
 
 // centroid = moment / (mass + (mass == 0)), as get_centroids divides
-__global__ void k_ctd_final2(double *ctd, const double *mom, const double *mass_c, long long n) {
+__global__ void k_ctd_final(double *ctd, const double *mom, const double *mass_c, long long n, int dim) {
     const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= n) return;
     const double d = mass_c[s] + (mass_c[s] == 0);
-    ctd[2 * s] = mom[2 * s] / d;
-    ctd[2 * s + 1] = mom[2 * s + 1] / d;
+    for (int k = 0; k < dim; ++k) ctd[dim * s + k] = mom[dim * s + k] / d;
 }
 
 }  // namespace
@@ -228,16 +226,16 @@ void rows_append(const Rows &dst, const Rows &src, long long n, unsigned *err, c
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
-void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
-                 const double *t_ctd, long long n, cudaStream_t st) {
+void accum_pass(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                const double *t_ctd, long long n, int dim, cudaStream_t st) {
     if (n <= 0) return;
-    k_accum2<<<ceil_div(n, TB), TB, 0, st>>>(mass, mass_c, mom, t_mass, t_mass_c, t_ctd, n);
+    k_accum<<<ceil_div(n, TB), TB, 0, st>>>(mass, mass_c, mom, t_mass, t_mass_c, t_ctd, n, dim);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
-void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st) {
+void centroids_final(double *ctd, const double *mom, const double *mass_c, long long n, int dim, cudaStream_t st) {
     if (n <= 0) return;
-    k_ctd_final2<<<ceil_div(n, TB), TB, 0, st>>>(ctd, mom, mass_c, n);
+    k_ctd_final<<<ceil_div(n, TB), TB, 0, st>>>(ctd, mom, mass_c, n, dim);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }

@@ -24,9 +24,9 @@ void csr_read_checks(unsigned long long out[3]);
 // divide the moments (get_centroids' mass + (mass == 0)).
 void rows_clear(const Rows &R, long long n, cudaStream_t st);
 void rows_append(const Rows &dst, const Rows &src, long long n, unsigned *err, cudaStream_t st);
-void accum_pass2(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
-                 const double *t_ctd, long long n, cudaStream_t st);
-void centroids_final2(double *ctd, const double *mom, const double *mass_c, long long n, cudaStream_t st);
+void accum_pass(double *mass, double *mass_c, double *mom, const double *t_mass, const double *t_mass_c,
+                const double *t_ctd, long long n, int dim, cudaStream_t st);
+void centroids_final(double *ctd, const double *mom, const double *mass_c, long long n, int dim, cudaStream_t st);
 // *count += number of i < n with m[i] == 0 (the empty cells)
 void count_zeros(const double *m, long long n, unsigned long long *count, cudaStream_t st);
 // out[idx[s] * d + k] = in[s * d + k]

@@ -658,9 +658,13 @@ template void pcg_bind<float>(PcgWorkT<float> &, double *, long long);
 
 namespace {
 
+// stall_checks > 0: also stop once |r|^2 has not halved over the last
+// stall_checks checks (the inner FP32 solves, whose attainable accuracy ends
+// above the tolerance on ill-conditioned systems).
 template <class M, class T>
 PcgResult pcg_run(const M &A, long long n, long long gauge_row, const T *b, T *x, double rel_tol, int max_iter,
-                  const PcgWorkT<T> &w, cudaStream_t st, int check, bool graph, bool multilevel) {
+                  const PcgWorkT<T> &w, cudaStream_t st, int check, bool graph, bool multilevel,
+                  int stall_checks = 0) {
     PcgResult res;
     if (n <= 0) {
         res.converged = true;
@@ -735,6 +739,8 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const T *b, T *x
         SDOT_CUDA(ie);
     }
     int it = 0;
+    double hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int nchecks = 0;
     while (it < max_iter) {
         const int chunk = check < max_iter - it ? check : max_iter - it;
         if (exec && chunk == check)
@@ -750,6 +756,12 @@ PcgResult pcg_run(const M &A, long long n, long long gauge_row, const T *b, T *x
         if (hs[S_RR] <= target) {
             res.converged = true;
             break;
+        }
+        if (stall_checks > 0) {
+            const int k = stall_checks < 8 ? stall_checks : 8;
+            if (nchecks >= k && !(hs[S_RR] <= 0.5 * hist[(nchecks - k) % 8])) break;
+            hist[nchecks % 8] = hs[S_RR];
+            ++nchecks;
         }
     }
     res.iterations = it;
@@ -909,7 +921,7 @@ PcgResult pcg_solve_refined(const Rows &rows, const float *val32, const float *s
             k_to_float<<<g, TB, 0, st>>>(r64, 1.0 / nr, b32, n);
             note_launch();
             const PcgResult in = pcg_run(A32, n, gauge_row, b32, d32, inner_tol, std::min(max_iter - it, 4000), w32,
-                                         st, check, st != nullptr, multilevel);
+                                         st, check, st != nullptr, multilevel, 4);
             it += in.iterations;
             res.levels = in.levels;
             k_add_scaled<float><<<g, TB, 0, st>>>(x, d32, nr, n);

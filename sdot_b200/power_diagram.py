@@ -220,7 +220,8 @@ class PowerDiagram:
         return out
 
     def solve_weights(self, target_masses, rel_mass_tol=1e-10, max_iter=150, damping=True, pcg_rel_tol=1e-12,
-                      pcg_max_iter=20000, verbosity=0, preconditioner="multilevel", linear_solver=None):
+                      pcg_max_iter=20000, verbosity=0, preconditioner="multilevel", linear_solver=None,
+                      raise_on_failure=True):
         """Newton on the weights so that every cell mass reaches its target
         (OptimalTransportSolver::solve, OptimalTransportSolver.tcc:27-119).
         Updates the weights of this diagram and returns the solver report as
@@ -228,7 +229,9 @@ class PowerDiagram:
         preconditioner: "multilevel" (V-cycle over Morton aggregates) or
         "jacobi".  linear_solver: "fp64" (FP64 PCG) or "fp32_refined" (FP32
         PCG with FP64 iterative refinement); by default "fp32_refined" for a
-        mixed-precision diagram and "fp64" otherwise."""
+        mixed-precision diagram and "fp64" otherwise.  raise_on_failure=False
+        returns the report (its "status" field set) instead of raising when the
+        tolerance is not reached."""
         t = _f64(target_masses, (self.nb_diracs,))
         if linear_solver is None:
             linear_solver = "fp32_refined" if self.precision == "mixed" else "fp64"
@@ -243,7 +246,8 @@ class PowerDiagram:
         self._weights = w
         report = {f: getattr(rep, f) for f, _ in rep._fields_}
         report["status"] = st
-        self._check(st)
+        if raise_on_failure or st not in (_lib.SDOT_OK, _lib.SDOT_NOT_CONVERGED):
+            self._check(st)
         return report
 
     def evaluate(self):

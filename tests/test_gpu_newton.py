@@ -242,7 +242,14 @@ def test_refined_newton_disc_clip_image(gpu_lib, ref_oracle):
     ref.set_image_density(c["image"])
     w_r, rep_r = newton.solve(ref, c["target"], c["weights"], tol=1e-12, ball_cut=True)
     assert rep_r["converged"]
-    assert np.abs(w_g - w_r).max() <= W_RTOL_REFINED * np.abs(w_r).max()
+    assert rep["max_rel_mass_error"] <= 1e-11
+    # with the disc clip there is no gauge fix: a uniform shift of the weights
+    # changes the masses only through the short arcs, so a 1e-11 mass error
+    # leaves the weights free along it; the weights agree once that shift is
+    # removed, and the shift itself is small
+    d = w_g - w_r
+    assert np.abs(d - d.mean()).max() <= 1e-10 * np.abs(w_r).max()
+    assert abs(d.mean()) <= 1e-7 * np.abs(w_r).max()
 
 
 def test_refined_newton_mirrored_clusters(gpu_lib):

@@ -128,3 +128,110 @@ def test_config4_density_newton(gpu_lib):
     assert np.max(np.abs(m - c["target"]) / c["target"]) <= 1e-8
     assert rep["iterations"] <= 20
     assert rep["pcg_levels"] >= 4  # the multilevel preconditioner ran (coarse rows of 128)
+
+
+# ---- 3D domains of other shapes (ConvexPolyhedronAssembly in 3D): convex
+# polyhedra given by (point, normal) pairs and tetrahedra, compared with the
+# compiled reference; several shapes (one pass per shape, summed) are
+# compared with the qhull oracle (oracle/poly3d.py), because the compiled
+# reference's 3D assembly of several shapes fails (segmentation fault in its
+# intersection of a cell with each shape) -- the qhull oracle is pinned to the
+# reference on single convex shapes in tests/test_oracle_poly3d.py
+def cube_corner_cut(shift=(0.0, 0.0, 0.0)):
+    """The unit cube with its corner x + y + z > 2.2 cut off (a tetrahedron
+    of legs 0.8), as 7 (point, outward normal) pairs."""
+    pts, nrm = [], []
+    for d in range(3):
+        for side in (0.0, 1.0):
+            q = [0.5, 0.5, 0.5]
+            q[d] = side
+            v = [0.0, 0.0, 0.0]
+            v[d] = 1.0 if side else -1.0
+            pts.append(q)
+            nrm.append(v)
+    pts.append([2.2 / 3] * 3)
+    nrm.append([1.0, 1.0, 1.0])
+    return np.array(pts) + np.asarray(shift), np.array(nrm)
+
+
+def test_convex_polyhedron_3d(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(302)
+    p = rng.random((3000, 3))
+    p = p[p.sum(1) < 2.15][:2500]
+    n = len(p)
+    pts, nrm = cube_corner_cut()
+    shapes = [("add_convex_polyhedron_shape", (pts, nrm, 1.0))]
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, shapes=shapes)
+    check_all(gpu, ref, n, rtol=RTOL, rtol_hess=1e-11)
+    assert abs(gpu.domain_measure() - (1 - 0.8 ** 3 / 6)) < 1e-13
+    assert abs(gpu.domain_measure() - ref.domain_measure()) < 1e-13
+
+
+def test_simplex_3d(gpu_lib, ref_oracle):
+    # the reference's 3D assembly has no simplex item: it is compared with the
+    # same tetrahedron given as four (point, normal) pairs
+    T = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    rng = np.random.default_rng(303)
+    p = rng.random((6000, 3))
+    p = p[p.sum(1) < 0.95][:600]
+    n = len(p)
+    from sdot_b200.power_diagram import PowerDiagram
+
+    gpu = PowerDiagram(p, np.zeros(n))
+    gpu.add_simplex_shape(T)
+    ref = ref_oracle.RefPowerDiagram(p, np.zeros(n))
+    pts = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [1.0, 0, 0]])
+    nrm = np.array([[-1.0, 0, 0], [0, -1.0, 0], [0, 0, -1.0], [1.0, 1.0, 1.0]])
+    ref.add_convex_polyhedron_shape(pts, nrm)
+    check_all(gpu, ref, n, rtol=RTOL, rtol_hess=1e-11)
+    assert abs(gpu.domain_measure() - 1.0 / 6.0) < 1e-15
+    assert abs(gpu.integrals().sum() - 1.0 / 6.0) < 1e-13
+
+
+def check_vs_poly3d(g, m_o, c_o, H_o):
+    m = g.integrals()
+    c = g.centroids()
+    off, col, val, _ = g.der_integrals_wrt_weights()
+    H = _dict_rows(off, col, val)
+    np.testing.assert_allclose(m, m_o, rtol=1e-11, atol=1e-12 * m_o.mean())
+    np.testing.assert_allclose(c, c_o, rtol=1e-11, atol=1e-12)
+    scale = max(abs(v) for v in H_o.values())
+    keys = set(H) | set(H_o)
+    worst = max(abs(H.get(k, 0.0) - H_o.get(k, 0.0)) for k in keys)
+    assert worst < 1e-11 * scale, worst
+
+
+def test_several_shapes_3d(gpu_lib):
+    from oracle import poly3d
+    from sdot_b200.power_diagram import PowerDiagram
+
+    rng = np.random.default_rng(304)
+    n = 600
+    p = rng.random((n, 3)) * [2.0, 1.0, 1.0]
+    pts, nrm = cube_corner_cut((1.0, 0.0, 0.0))
+    g = PowerDiagram(p, np.zeros(n))
+    g.add_box_shape([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], coeff=1.0)
+    g.add_convex_polyhedron_shape(pts, nrm, coeff=2.0)
+    nn = nrm / np.linalg.norm(nrm, axis=1)[:, None]
+    planes = np.hstack([nn, np.sum(nn * pts, 1)[:, None]])
+    lo, hi = pts.min(0), pts.max(0)
+    shapes = [((0, 0, 0), (1, 1, 1), None, 1.0), (lo - (hi - lo), hi + (hi - lo), planes, 2.0)]
+    m_o, c_o, H_o = poly3d.integrate_shapes(p, shapes)
+    check_vs_poly3d(g, m_o, c_o, H_o)
+    assert abs(g.domain_measure() - (1.0 + 2.0 * (1 - 0.8 ** 3 / 6))) < 1e-13
+
+
+def test_two_boxes_3d_density(gpu_lib):
+    from oracle import poly3d
+    from sdot_b200.power_diagram import PowerDiagram
+
+    rng = np.random.default_rng(305)
+    n = 500
+    p = rng.random((n, 3)) * [2.0, 1.0, 1.0]
+    g = PowerDiagram(p, np.zeros(n))
+    g.add_box_shape([0.0, 0.0, 0.0], [1.0, 1.0, 1.0], coeff=1.0)
+    g.add_box_shape([1.0, 0.0, 0.0], [2.0, 1.0, 1.0], coeff=0.5)
+    g.set_polynomial_density(workloads.C4_DENSITY)
+    shapes = [((0, 0, 0), (1, 1, 1), None, 1.0), ((1, 0, 0), (2, 1, 1), None, 0.5)]
+    m_o, c_o, H_o = poly3d.integrate_shapes(p, shapes, poly=workloads.C4_DENSITY)
+    check_vs_poly3d(g, m_o, c_o, H_o)

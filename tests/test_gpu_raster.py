@@ -66,11 +66,14 @@ def test_image_of_cell_nums(gpu_lib, ref_oracle):
     r = ref.image_of_cell_nums([0.0, 0.0], [1.0, 1.0], nbp)
     assert ((g < 0) == (r < 0)).all()
     assert (g >= r).all()
-    # where they differ, the pixel meets two cells (pixels are ~1/100 of a
-    # cell): the GPU's cell is then a neighbour of the reference's one
+    # where they differ, the pixel meets several cells (pixels are ~1/100 of
+    # a cell): the GPU's cell is then a neighbour of the reference's one, or
+    # a neighbour of one of its neighbours (a pixel over a short edge meets
+    # the two cells on either side of it, which do not touch)
     off, ids = ref.neighbors()
+    nb = [set(int(j) for j in ids[off[i]:off[i + 1]] if j >= 0) for i in range(n)]
     diff = np.argwhere(g != r)
     assert len(diff) < 0.2 * g.size
     for iy, ix in diff:
         a, b = int(r[iy, ix]), int(g[iy, ix])
-        assert b in set(ids[off[a]:off[a + 1]].tolist()), (iy, ix, a, b)
+        assert b in nb[a] or any(b in nb[k] for k in nb[a]), (iy, ix, a, b)

@@ -82,3 +82,44 @@ def test_density_one_matches_the_compiled_reference(ref_oracle):
     keys = set(RH) | set(H)
     worst = max(abs(RH.get(k, 0.0) - H.get(k, 0.0)) for k in keys)
     assert worst < 1e-10 * scale, worst
+
+
+def test_convex_shape_planes_vs_reference(ref_oracle):
+    # the half-space extension of the qhull oracle (a convex shape: its box
+    # cut by planes) against the compiled reference on one convex shape
+    from oracle import poly3d
+
+    rng = np.random.default_rng(307)
+    p = rng.random((2000, 3))
+    p = p[p.sum(1) < 2.15][:300]
+    n = len(p)
+    pts, nrm = [], []
+    for d in range(3):
+        for side in (0.0, 1.0):
+            q = [0.5, 0.5, 0.5]
+            q[d] = side
+            v = [0.0, 0.0, 0.0]
+            v[d] = 1.0 if side else -1.0
+            pts.append(q)
+            nrm.append(v)
+    pts.append([2.2 / 3] * 3)
+    nrm.append([1.0, 1.0, 1.0])
+    pts, nrm = np.array(pts), np.array(nrm)
+    r = ref_oracle.RefPowerDiagram(p, np.zeros(n))
+    r.add_convex_polyhedron_shape(pts, nrm)
+    m_r = r.integrals()
+    c_r = r.centroids()
+    nn = nrm / np.linalg.norm(nrm, axis=1)[:, None]
+    planes = np.hstack([nn, np.sum(nn * pts, 1)[:, None]])
+    lo, hi = pts.min(0), pts.max(0)
+    m_o, c_o, H_o = poly3d.integrate(p, lo=lo - (hi - lo), hi=hi + (hi - lo), planes=planes)
+    np.testing.assert_allclose(m_o, m_r, rtol=1e-11, atol=1e-12 * m_r.mean())
+    np.testing.assert_allclose(c_o, c_r, rtol=1e-11, atol=1e-12)
+    _, off, col, val, _ = r.der_integrals_wrt_weights()
+    H_r = {}
+    for i in range(n):
+        for k in range(off[i], off[i + 1]):
+            H_r[(i, int(col[k]))] = H_r.get((i, int(col[k])), 0.0) + val[k]
+    scale = max(abs(v) for v in H_r.values())
+    keys = set(H_r) | set(H_o)
+    assert max(abs(H_r.get(k, 0.0) - H_o.get(k, 0.0)) for k in keys) < 1e-10 * scale
