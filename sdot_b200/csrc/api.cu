@@ -106,6 +106,10 @@ struct HostPoly3 {
     // keeps a . x <= b
     void cut(const double *a, double b) {
         auto d = [&](const P3 &v) { return a[0] * v[0] + a[1] * v[1] + a[2] * v[2] - b; };
+        bool removes = false;  // a plane that only touches the polyhedron changes nothing
+        for (const auto &f : faces)
+            for (const P3 &v : f) removes |= d(v) > 0;
+        if (!removes) return;
         std::vector<std::vector<P3>> out;
         std::vector<P3> cap;  // points on the plane: the new face
         for (const auto &f : faces) {

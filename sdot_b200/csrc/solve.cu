@@ -79,6 +79,46 @@ struct RowsMatT {
 using RowsMat = RowsMatT<double>;
 inline RowsMat rows_mat(const Rows &R) { return RowsMat{R, R.val, R.side_val}; }
 
+// The FP32 copy of the Hessian rows in Laplacian form: an off-diagonal entry
+// holds the edge weight w_sj = -a_sj, the diagonal entry the row sum r_s (the
+// part of the diagonal that is not the sum of the edge weights: disc arcs),
+// so that (A x)_s = r_s x_s + sum_j w_sj (x_s - x_j).  Rounding the weights to
+// FP32 then perturbs each edge by a relative 6e-8, which bounds the FP32
+// operator between (1 -+ 6e-8) times the exact one; rounding the entries
+// themselves would break the zero row sums by 6e-8 of the diagonal, far
+// above the smallest eigenvalues of these systems.  Sums in double.
+struct RowsLap32 {
+    Rows R;
+    const float *val;
+    const float *side_val;
+    __device__ int len(long long s) const { return R.cnt[s]; }
+    __device__ long long colk(long long s, int k) const { return *R.colp(s, k); }
+    __device__ double raw(long long s, int k) const {
+        return R.cnt[s] > R.cap ? double(side_val[R.side[s] + k]) : double(val[k * R.stride + s]);
+    }
+    template <class F>
+    __device__ double row_sum(long long s, const F &f) const {
+        const int m = R.cnt[s];
+        const double fs = f(s);
+        double acc = 0;
+        for (int k = 0; k < m; ++k) {
+            const long long c = colk(s, k);
+            acc += c == s ? raw(s, k) * fs : raw(s, k) * (fs - f(c));
+        }
+        return acc;
+    }
+    template <class X>
+    __device__ double row_dot(long long s, const X *x) const {
+        return row_sum(s, [&](long long j) { return double(x[j]); });
+    }
+    __device__ double diag(long long s) const {
+        double d = 0;
+        for (int k = 0, m = R.cnt[s]; k < m; ++k) d += raw(s, k);  // r_s + sum of the weights
+        return d;
+    }
+    __device__ double valk(long long s, int k) const { return colk(s, k) == s ? diag(s) : -raw(s, k); }
+};
+
 struct CsrView {
     CsrMat M;
     template <class X>
@@ -380,9 +420,9 @@ __global__ void k_mg_coarsen(M A, long long nf, long long gauge, const double *s
 // Pre-smoothing and restriction of one level: z = w D^-1 r, and
 // rc[aggregate] = sum over its rows of (r - A z).  Rows are taken a block at a
 // time so that the MG_B rows of an aggregate sit in consecutive lanes.
-template <class M, class T>
+template <class M, class T, class TC>
 __global__ void k_mg_pre(M A, long long n, long long gauge, const double *scal, const T *dinv, const T *r, T *z,
-                         T *rc) {
+                         TC *rc) {
     const unsigned FULL = 0xffffffffu;
     for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
         const long long i = i0 + threadIdx.x;
@@ -396,16 +436,16 @@ __global__ void k_mg_pre(M A, long long n, long long gauge, const double *scal, 
             t = ri - acc;
         }
         for (int o = MG_B / 2; o > 0; o >>= 1) t += __shfl_down_sync(FULL, t, o, MG_B);
-        if ((threadIdx.x & (MG_B - 1)) == 0 && i < n) rc[i / MG_B] = T(t);
+        if ((threadIdx.x & (MG_B - 1)) == 0 && i < n) rc[i / MG_B] = TC(t);
     }
 }
 
 // Coarse correction and post-smoothing: z' = z + P zc, zo = z' + w D^-1 (r - A z').
 // On the finest level (FINE) it also sums r . zo per block into partial[]
 // and, when p is given, writes p = zo (the first CG direction).
-template <class M, bool FINE, class T>
+template <class M, bool FINE, class T, class TC>
 __global__ void k_mg_post(M A, long long n, long long gauge, const double *scal, const T *dinv, const T *r, const T *z,
-                          const T *zc, T *zo, double *partial, T *p) {
+                          const TC *zc, T *zo, double *partial, T *p) {
     __shared__ double sh[32];
     double rz = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -531,7 +571,7 @@ constexpr int MG_MAX_LEV = 16;
 template <class T>
 struct MgPlan {
     int L = 0;                        // coarse levels 1..L (level L is the coarsest)
-    MgLevelT<T> lev[MG_MAX_LEV + 1];  // lev[0]: the fine level (n only)
+    MgLevelT<double> lev[MG_MAX_LEV + 1];  // lev[0]: the fine level (n only); coarse levels in FP64
     double *cinv = nullptr;           // coarsest dense inverse
     int *flag = nullptr;              // coarse-row overflow
 };
@@ -554,13 +594,13 @@ size_t mg_plan(long long n, int cap, double *base, MgPlan<T> &pl) {
     long long m = n;
     while (m > MG_COARSE && pl.L < MG_MAX_LEV) {
         m = (m + MG_B - 1) / MG_B;
-        MgLevelT<T> &v = pl.lev[++pl.L];
+        MgLevelT<double> &v = pl.lev[++pl.L];
         v.n = m;
-        v.val = take(size_t(cap) * m, (T *)nullptr);
-        v.dinv = take(m, (T *)nullptr);
-        v.r = take(m, (T *)nullptr);
-        v.z = take(m, (T *)nullptr);
-        v.zo = take(m, (T *)nullptr);
+        v.val = take(size_t(cap) * m, (double *)nullptr);
+        v.dinv = take(m, (double *)nullptr);
+        v.r = take(m, (double *)nullptr);
+        v.z = take(m, (double *)nullptr);
+        v.zo = take(m, (double *)nullptr);
         v.cnt = take(m, (int *)nullptr);
         v.col = take(size_t(cap) * m, (int *)nullptr);
     }
@@ -576,8 +616,7 @@ int coarse_grid(long long n) {
     return int(g < 148 * 8 ? (g < 1 ? 1 : g) : 148 * 8);
 }
 
-template <class T>
-EllViewT<T> ell(const MgLevelT<T> &v) { return EllViewT<T>{v.cnt, v.col, v.val, v.n}; }
+inline EllViewT<double> ell(const MgLevelT<double> &v) { return EllViewT<double>{v.cnt, v.col, v.val, v.n}; }
 
 // Builds the coarse levels of A; false when a coarse row outgrew MG_CAP.
 template <class M, int SLOTS, class T>
@@ -585,9 +624,9 @@ void mg_coarsen_all(const M &A, long long gauge, const double *scal, const MgPla
     for (int l = 1; l <= pl.L; ++l) {
         const int g = coarse_grid(32 * pl.lev[l].n);  // one warp per coarse row
         if (l == 1)
-            k_mg_coarsen<M, SLOTS, T><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
+            k_mg_coarsen<M, SLOTS, double><<<g, TB, 0, st>>>(A, pl.lev[0].n, gauge, scal, pl.lev[1], pl.flag);
         else
-            k_mg_coarsen<EllViewT<T>, SLOTS, T><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal,
+            k_mg_coarsen<EllViewT<double>, SLOTS, double><<<g, TB, 0, st>>>(ell(pl.lev[l - 1]), pl.lev[l - 1].n, -1, scal,
                                                                   pl.lev[l], pl.flag);
         note_launch();
     }
@@ -600,7 +639,7 @@ bool mg_setup(const M &A, long long gauge, const double *scal, const MgPlan<T> &
         mg_coarsen_all<M, 4>(A, gauge, scal, pl, st);
     else
         mg_coarsen_all<M, 2>(A, gauge, scal, pl, st);
-    k_mg_coarsest_setup<T><<<1, MG_COARSE, 0, st>>>(ell(pl.lev[pl.L]), int(pl.lev[pl.L].n), pl.cinv);
+    k_mg_coarsest_setup<double><<<1, MG_COARSE, 0, st>>>(ell(pl.lev[pl.L]), int(pl.lev[pl.L].n), pl.cinv);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
     int flag = 0;
@@ -615,20 +654,20 @@ template <class M, class T>
 void mg_vcycle(const M &A, long long gauge, const double *scal, const T *dinv0, const MgPlan<T> &pl, const T *r0,
                T *zpre0, T *z0, double *partial, T *p0, int g, cudaStream_t st) {
     const long long n = pl.lev[0].n;
-    k_mg_pre<M, T><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].r);
+    k_mg_pre<M, T, double><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].r);
     for (int l = 1; l < pl.L; ++l) {
-        const MgLevelT<T> &v = pl.lev[l];
-        k_mg_pre<EllViewT<T>, T><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
+        const MgLevelT<double> &v = pl.lev[l];
+        k_mg_pre<EllViewT<double>, double, double><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
                                                                    pl.lev[l + 1].r);
     }
-    const MgLevelT<T> &c = pl.lev[pl.L];
-    k_mg_coarsest_apply<T><<<1, MG_COARSE, 0, st>>>(pl.cinv, int(c.n), c.r, c.zo);
+    const MgLevelT<double> &c = pl.lev[pl.L];
+    k_mg_coarsest_apply<double><<<1, MG_COARSE, 0, st>>>(pl.cinv, int(c.n), c.r, c.zo);
     for (int l = pl.L - 1; l >= 1; --l) {
-        const MgLevelT<T> &v = pl.lev[l];
-        k_mg_post<EllViewT<T>, false, T><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
+        const MgLevelT<double> &v = pl.lev[l];
+        k_mg_post<EllViewT<double>, false, double, double><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
                                                                            pl.lev[l + 1].zo, v.zo, nullptr, nullptr);
     }
-    k_mg_post<M, true, T><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].zo, z0, partial, p0);
+    k_mg_post<M, true, T, double><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].zo, z0, partial, p0);
 }
 
 template <class T>
@@ -813,14 +852,21 @@ void gather_sorted(const double *t_orig, const int *idx, double *t_sorted, long 
 // ---- FP32 solves with FP64 iterative refinement ---------------------------
 namespace {
 
-__global__ void k_rows_to_float(Rows R, long long n, float *val32, float *side32, const unsigned long long *side_used) {
-    const long long total = (long long)R.cap * R.stride;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
-        if (i % R.stride < n) val32[i] = float(R.val[i]);
-    const long long ns = side_used ? (long long)*side_used : 0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns && i < R.side_cap;
-         i += (long long)gridDim.x * blockDim.x)
-        side32[i] = float(R.side_val[i]);
+// the Laplacian form of RowsLap32, one thread per row
+__global__ void k_rows_to_float(Rows R, long long n, float *val32, float *side32) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const int m = R.cnt[s];
+        double rs = 0;
+        for (int k = 0; k < m; ++k) rs += *R.valp(s, k);
+        const bool side = m > R.cap;
+        for (int k = 0; k < m; ++k) {
+            const float v = float(*R.colp(s, k) == s ? rs : -*R.valp(s, k));
+            if (side)
+                side32[R.side[s] + k] = v;
+            else
+                val32[k * R.stride + s] = v;
+        }
+    }
 }
 
 // partial[block] = sum of v^2 over the block's entries
@@ -877,7 +923,7 @@ double sumsq(const double *v, long long n, double *partial, double *dev_out, cud
 
 void rows_to_float(const Rows &rows, long long n, float *val32, float *side_val32, cudaStream_t st) {
     if (n <= 0) return;
-    k_rows_to_float<<<PCG_BLOCKS, TB, 0, st>>>(rows, n, val32, side_val32, rows.side_used);
+    k_rows_to_float<<<PCG_BLOCKS, TB, 0, st>>>(rows, n, val32, side_val32);
     note_launch();
     SDOT_CUDA(cudaGetLastError());
 }
@@ -892,7 +938,7 @@ PcgResult pcg_solve_refined(const Rows &rows, const float *val32, const float *s
         return res;
     }
     const RowsMat A64 = rows_mat(rows);
-    const RowsMatT<float> A32{rows, val32, side_val32};
+    const RowsLap32 A32{rows, val32, side_val32};
     const int g = grid_of(n);
     double *r64 = res64;                                        // n doubles: the FP64 residual
     float *b32 = reinterpret_cast<float *>(res64 + n);          // n floats: the scaled residual

@@ -78,8 +78,8 @@ PcgResult pcg_solve_refined(const Rows &rows, const float *val32, const float *s
                             long long gauge_row, const double *b, double *x, double rel_tol, int max_iter,
                             const PcgWork &w64, const PcgWorkT<float> &w32, double *res64, cudaStream_t st,
                             double inner_tol = 1e-5, int check = 32, bool multilevel = true);
-// FP32 copies of the rows' values (ELL slots of the first n rows and the side
-// buffer's side_used entries).
+// FP32 copy of the rows' values in Laplacian form (off-diagonal entries:
+// the edge weights -a_sj; diagonal entry: the row sum), same layout.
 void rows_to_float(const Rows &rows, long long n, float *val32, float *side_val32, cudaStream_t st);
 
 // The same solve on a CSR matrix (device arrays: off[n + 1], col[nnz], val[nnz]).

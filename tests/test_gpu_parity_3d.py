@@ -180,7 +180,9 @@ def test_simplex_3d(gpu_lib, ref_oracle):
     gpu = PowerDiagram(p, np.zeros(n))
     gpu.add_simplex_shape(T)
     ref = ref_oracle.RefPowerDiagram(p, np.zeros(n))
-    pts = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [1.0, 0, 0]])
+    # one point on each face plane; together they span the tetrahedron's box,
+    # which the reference inflates and cuts by the four planes
+    pts = np.array([[0, 1.0, 0], [0, 0, 1.0], [1.0, 0, 0], [1.0, 0, 0]])
     nrm = np.array([[-1.0, 0, 0], [0, -1.0, 0], [0, 0, -1.0], [1.0, 1.0, 1.0]])
     ref.add_convex_polyhedron_shape(pts, nrm)
     check_all(gpu, ref, n, rtol=RTOL, rtol_hess=1e-11)
