@@ -234,8 +234,9 @@ struct sdot_ctx {
     bool has_poly = false;     // 3D multilinear density factor
     double poly3[8] = {1, 0, 0, 0, 0, 0, 0, 0};
     bool has_image = false;
-    double img_lo[2] = {0, 0}, img_hi[2] = {1, 1};
-    long long img_size[2] = {0, 0};
+    double img_lo[3] = {0, 0, 0}, img_hi[3] = {1, 1, 1};
+    long long img_size[3] = {1, 1, 1};
+    char *img_backup3 = nullptr;  // 3D voxel images: the kernels' per-warp face copies
     int img_ncoeffs = 1;
     std::vector<double> img_data;
     int ball = 0;
@@ -305,6 +306,7 @@ struct sdot_ctx {
         dfree(d_start); dfree(d_img); dfree(d_item_xy); dfree(d_item_nrm); dfree(d_item_coeff); dfree(d_item_off);
         dfree(d_trans);
         dfree(d_planes3);
+        dfree(img_backup3);
         free_eval();
         free_newton();
         free_multi();
@@ -484,6 +486,17 @@ struct sdot_ctx {
 
     // the domain is one the kernels handle; uploads the 2D one
     void check_domain() {
+        if (dim == 3 && has_image) {
+            if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
+            if (has_poly) throw Unsupported("a multilinear density factor with a voxel image is not available");
+            if (dom_dirty) {
+                dalloc(d_img, img_data.size());
+                SDOT_CUDA(cudaMemcpy(d_img, img_data.data(), img_data.size() * sizeof(double), cudaMemcpyHostToDevice));
+                if (!img_backup3) dalloc(img_backup3, cells3d_image_backup_bytes());
+                dom_dirty = false;
+            }
+            return;
+        }
         if (dim == 3) {
             if (items3.empty()) throw BadArg("no domain: call sdot_add_box_shape (or another add_..._shape) first");
             if (ball) throw Unsupported("no ball cut in 3D (the reference's ConvexPolyhedron3::ball_cut is a TODO)");
@@ -591,7 +604,16 @@ struct sdot_ctx {
         a.w = tree3.w;
         a.nodes = tree3.nodes;
         a.max_nodes = tree3.max_nodes;
-        if (k >= 0) {
+        if (has_image) {
+            // ScaledImage: the cells start from the image box
+            for (int d = 0; d < 3; ++d) {
+                a.box_lo[d] = a.img_lo[d] = img_lo[d];
+                a.box_hi[d] = a.img_hi[d] = img_hi[d];
+                a.img_n[d] = int(img_size[d]);
+            }
+            a.img = d_img;
+            a.img_backup = img_backup3;
+        } else if (k >= 0) {
             for (int d = 0; d < 3; ++d) {
                 a.box_lo[d] = items3[k].lo[d];
                 a.box_hi[d] = items3[k].hi[d];
@@ -656,7 +678,7 @@ struct sdot_ctx {
         SDOT_CUDA(cudaEventRecord(ev[0], stream));
         ensure_tree();
         SDOT_CUDA(cudaEventRecord(ev[1], stream));
-        if (dim == 3 && items3.size() > 1) {
+        if (dim == 3 && items3.size() > 1 && !has_image) {
             evaluate_multi3();
         } else if (dim == 3) {
             Cell3DArgs a = args3(0);
@@ -760,8 +782,9 @@ struct sdot_ctx {
             SDOT_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), stream));
             if (dim == 3) {
                 // several shapes: the traversal cell in the englobing box
-                Cell3DArgs a = args3(items3.size() > 1 ? -1 : 0);
-                if (items3.size() > 1) {
+                Cell3DArgs a = args3(items3.size() > 1 && !has_image ? -1 : 0);
+                a.img = nullptr;  // the traversal cell, before any intersection
+                if (items3.size() > 1 && !has_image) {
                     a.hint = nullptr;
                     a.use_hint = 0;
                 }
@@ -1350,19 +1373,23 @@ int sdot_set_image_density(sdot_ctx *ctx, const double *min_pt, const double *ma
                            const int64_t *sizes, int nb_coeffs) {
     return guarded(ctx, [&] {
         if (!min_pt || !max_pt || !data || !sizes) throw BadArg("null image argument");
-        if (ctx->dim != 2) throw Unsupported("in 3D only box domains are available in this build");
-        if (nb_coeffs != 1 && nb_coeffs != 6)
-            throw Unsupported("images have nb_coeffs = 1 (piecewise constant) or 6 (piecewise quadratic)");
-        if (sizes[0] <= 0 || sizes[1] <= 0) throw BadArg("bad image size");
+        if (nb_coeffs != 1 && !(nb_coeffs == 6 && ctx->dim == 2))
+            throw Unsupported("images have nb_coeffs = 1 (piecewise constant), or 6 (piecewise quadratic) in 2D "
+                              "(Polynomial.h:53-58)");
+        long long np = 1;
+        for (int d = 0; d < ctx->dim; ++d) {
+            if (sizes[d] <= 0 || sizes[d] > (1 << 30)) throw BadArg("bad image size");
+            np *= sizes[d];
+        }
         ctx->items.clear();
         ctx->has_image = true;
-        for (int d = 0; d < 2; ++d) {
-            ctx->img_lo[d] = min_pt[d];
-            ctx->img_hi[d] = max_pt[d];
-            ctx->img_size[d] = sizes[d];
+        for (int d = 0; d < 3; ++d) {
+            ctx->img_lo[d] = d < ctx->dim ? min_pt[d] : 0.0;
+            ctx->img_hi[d] = d < ctx->dim ? max_pt[d] : 1.0;
+            ctx->img_size[d] = d < ctx->dim ? sizes[d] : 1;
         }
         ctx->img_ncoeffs = nb_coeffs;
-        ctx->img_data.assign(data, data + sizes[0] * sizes[1] * nb_coeffs);
+        ctx->img_data.assign(data, data + np * nb_coeffs);
         ctx->dom_dirty = true;
         ctx->mark_dirty();
         return int(SDOT_OK);
@@ -1402,7 +1429,7 @@ static double domain_measure(const sdot_ctx *ctx) {
     if (ctx->has_image) {
         // ScaledImage::measure (ScaledImage.tcc:36-69): the mean over the
         // pixels of the density's average on the pixel, times the area
-        const long long nx = ctx->img_size[0], ny = ctx->img_size[1], np = nx * ny;
+        const long long nx = ctx->img_size[0], ny = ctx->img_size[1], np = nx * ny * ctx->img_size[2];
         double s = 0;
         if (ctx->img_ncoeffs == 6) {
             // average of c0 + c1 x + c2 y + c3 x^2 + c4 xy + c5 y^2 on a pixel
@@ -1423,7 +1450,7 @@ static double domain_measure(const sdot_ctx *ctx) {
             for (double v : ctx->img_data) s += v;
         }
         s /= double(np);
-        for (int d = 0; d < 2; ++d) s *= ctx->img_hi[d] - ctx->img_lo[d];
+        for (int d = 0; d < ctx->dim; ++d) s *= ctx->img_hi[d] - ctx->img_lo[d];
         return s;
     }
     double res = 0;

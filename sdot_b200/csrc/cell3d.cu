@@ -378,11 +378,177 @@ __device__ void guard_fail3(const Cell3DArgs &A, int code, long long s, long lon
     flag_error(A.err, DE_GUARD);
 }
 
+// Volume, first moments (relative to c0) and per face slot the area of the
+// faces of C, the pyramids of apex c0 over the faces (this lane's slots only;
+// the caller sums over the warp).  Constant density.
+template <int FPL, int MAXV>
+__device__ void face_volumes(const Cell3<FPL, MAXV> &C, double &vol, double &mx, double &my, double &mz,
+                             double *area_r) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        const int n = C.nv[r];
+        area_r[r] = 0;
+        if (n < 3) continue;
+        const double na = sqrt(C.ax[r] * C.ax[r] + C.ay[r] * C.ay[r] + C.az[r] * C.az[r]);
+        const double ux = C.ax[r] / na, uy = C.ay[r] / na, uz = C.az[r] / na;
+        const int i0 = C.F.at(0, f);
+        const double x0 = C.F.X[i0], y0 = C.F.Y[i0], z0 = C.F.Z[i0];
+        double area = 0, fx = 0, fy = 0, fz = 0;
+        for (int k = 1; k + 1 < n; ++k) {
+            const int i1 = C.F.at(k, f), i2 = C.F.at(k + 1, f);
+            const double e1x = C.F.X[i1] - x0, e1y = C.F.Y[i1] - y0, e1z = C.F.Z[i1] - z0;
+            const double e2x = C.F.X[i2] - x0, e2y = C.F.Y[i2] - y0, e2z = C.F.Z[i2] - z0;
+            const double ta =
+                0.5 * ((e1y * e2z - e1z * e2y) * ux + (e1z * e2x - e1x * e2z) * uy + (e1x * e2y - e1y * e2x) * uz);
+            area += ta;
+            fx += ta * (3 * x0 + e1x + e2x);
+            fy += ta * (3 * y0 + e1y + e2y);
+            fz += ta * (3 * z0 + e1z + e2z);
+        }
+        const double h = C.b[r] / na;
+        const double v = h * area / 3;
+        vol += v;
+        if (area != 0) {
+            const double k = v * 0.75 / (3 * area);
+            mx += k * fx;
+            my += k * fy;
+            mz += k * fz;
+        }
+        area_r[r] = area;
+    }
+}
+
+// The cell integrated voxel by voxel (ScaledImage::for_each_intersection,
+// ScaledImage.tcc:98-149: each voxel box intersected with the cell and
+// integrated with the voxel's value): the faces are saved to the warp's
+// backup, and for every voxel that the cell's bounding box meets the faces
+// are restored and cut by the voxel's six planes, then integrated.  Sums
+// (this lane's slots) into vol, m*, and per slot the value-weighted area of
+// the Dirac faces.  Returns 0, or 1 / 2 as cut3 (capacity, degenerate).
+template <int FPL, int MAXV>
+__device__ int voxel_integrals(const Cell3DArgs &A, Cell3<FPL, MAXV> &C, char *backup, double c0x, double c0y,
+                               double c0z, double &vol, double &mx, double &my, double &mz, double *wa_r) {
+    const int lane = threadIdx.x & 31;
+    Faces<FPL, MAXV> B;
+    constexpr int MAXF = 32 * FPL;
+    B.X = reinterpret_cast<double *>(backup);
+    B.Y = B.X + MAXV * MAXF;
+    B.Z = B.Y + MAXV * MAXF;
+    B.E = reinterpret_cast<int *>(B.Z + MAXV * MAXF);
+    int fid0[FPL], nv0[FPL];
+    double ax0[FPL], ay0[FPL], az0[FPL], b0[FPL];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        fid0[r] = C.fid[r];
+        nv0[r] = C.nv[r];
+        ax0[r] = C.ax[r];
+        ay0[r] = C.ay[r];
+        az0[r] = C.az[r];
+        b0[r] = C.b[r];
+        wa_r[r] = 0;
+        for (int v = 0; v < C.nv[r]; ++v) {
+            const int i = C.F.at(v, f);
+            B.X[i] = C.F.X[i];
+            B.Y[i] = C.F.Y[i];
+            B.Z[i] = C.F.Z[i];
+            B.E[i] = C.F.E[i];
+            lo[0] = fmin(lo[0], C.F.X[i]); hi[0] = fmax(hi[0], C.F.X[i]);
+            lo[1] = fmin(lo[1], C.F.Y[i]); hi[1] = fmax(hi[1], C.F.Y[i]);
+            lo[2] = fmin(lo[2], C.F.Z[i]); hi[2] = fmax(hi[2], C.F.Z[i]);
+        }
+    }
+    for (int d = 0; d < 3; ++d)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[d] = fmin(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+            hi[d] = fmax(hi[d], __shfl_xor_sync(FULL, hi[d], o));
+        }
+    __syncwarp();
+    if (!(lo[0] <= hi[0])) return 0;  // an empty cell
+    const double c0[3] = {c0x, c0y, c0z};
+    int i0[3], i1[3];
+    double ps[3];
+    for (int d = 0; d < 3; ++d) {
+        ps[d] = (A.img_hi[d] - A.img_lo[d]) / A.img_n[d];
+        i0[d] = max(0, int(floor((lo[d] + c0[d] - A.img_lo[d]) / ps[d])));
+        i1[d] = min(A.img_n[d] - 1, int(floor((hi[d] + c0[d] - A.img_lo[d]) / ps[d])));
+    }
+    for (int iz = i0[2]; iz <= i1[2]; ++iz)
+        for (int iy = i0[1]; iy <= i1[1]; ++iy)
+            for (int ix = i0[0]; ix <= i1[0]; ++ix) {
+                const double val = A.img[((long long)iz * A.img_n[1] + iy) * A.img_n[0] + ix];
+                // restore the cell
+#pragma unroll
+                for (int r = 0; r < FPL; ++r) {
+                    const int f = lane + 32 * r;
+                    C.fid[r] = fid0[r];
+                    C.nv[r] = nv0[r];
+                    C.ax[r] = ax0[r];
+                    C.ay[r] = ay0[r];
+                    C.az[r] = az0[r];
+                    C.b[r] = b0[r];
+                    for (int v = 0; v < nv0[r]; ++v) {
+                        const int i = C.F.at(v, f);
+                        C.F.X[i] = B.X[i];
+                        C.F.Y[i] = B.Y[i];
+                        C.F.Z[i] = B.Z[i];
+                        C.F.E[i] = B.E[i];
+                    }
+                }
+                __syncwarp();
+                // the voxel's six planes, relative to c0
+                const int ii[3] = {ix, iy, iz};
+                for (int d = 0; d < 3; ++d) {
+                    const double vlo = A.img_lo[d] + ps[d] * ii[d] - c0[d];
+                    const double vhi = A.img_lo[d] + ps[d] * (ii[d] + 1) - c0[d];
+                    double a[3] = {0, 0, 0};
+                    a[d] = -1.0;
+                    int st = cut3(C, a[0], a[1], a[2], -vlo, domain_id(200 + 2 * d));
+                    if (st) return st;
+                    a[d] = 1.0;
+                    st = cut3(C, a[0], a[1], a[2], vhi, domain_id(201 + 2 * d));
+                    if (st) return st;
+                }
+                double v = 0, px = 0, py = 0, pz = 0, ar[FPL];
+                face_volumes(C, v, px, py, pz, ar);
+                vol += val * v;
+                mx += val * px;
+                my += val * py;
+                mz += val * pz;
+#pragma unroll
+                for (int r = 0; r < FPL; ++r)
+                    if (C.fid[r] >= 0 && C.nv[r] >= 3) wa_r[r] += val * ar[r];
+            }
+    // restore the cell for the outputs that follow (its faces' ids and planes)
+#pragma unroll
+    for (int r = 0; r < FPL; ++r) {
+        const int f = lane + 32 * r;
+        C.fid[r] = fid0[r];
+        C.nv[r] = nv0[r];
+        C.ax[r] = ax0[r];
+        C.ay[r] = ay0[r];
+        C.az[r] = az0[r];
+        C.b[r] = b0[r];
+        for (int v = 0; v < nv0[r]; ++v) {
+            const int i = C.F.at(v, f);
+            C.F.X[i] = B.X[i];
+            C.F.Y[i] = B.Y[i];
+            C.F.Z[i] = B.Z[i];
+            C.F.E[i] = B.E[i];
+        }
+    }
+    __syncwarp();
+    return 0;
+}
+
 // Builds and integrates the cell of sorted Dirac s.  Returns 0 (outputs
 // written), 1 (a capacity was exceeded: retry in the large pass), 2 (failed:
 // outputs written as NaN / empty row, error flagged).
 template <int FPL, int MAXV>
-__device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
+__device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C, char *backup) {
     const int lane = threadIdx.x & 31;
     const double c0x = A.pos[3 * s], c0y = A.pos[3 * s + 1], c0z = A.pos[3 * s + 2], w0 = A.w[s];
     init_box(C, A, c0x, c0y, c0z);
@@ -492,6 +658,11 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
     int rpos[FPL], npos[FPL];
     double rval[FPL];
     bool rmine[FPL], nmine[FPL];
+    double img_area[FPL];  // voxel image: the value-weighted area of each Dirac face
+    if (status == 0 && A.img) {
+        status = voxel_integrals(A, C, backup, c0x, c0y, c0z, vol, mx, my, mz, img_area);
+        if (status == 1) return 1;
+    }
     if (status == 0) {
         const bool poly = A.has_poly;
         const PolyRel pr(A.poly, c0x, c0y, c0z);
@@ -504,6 +675,16 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C) {
             rval[r] = 0;
             if (n < 3) continue;
             const double na = sqrt(C.ax[r] * C.ax[r] + C.ay[r] * C.ay[r] + C.az[r] * C.az[r]);
+            if (A.img) {
+                // integrated voxel by voxel above
+                if (C.fid[r] >= 0) {
+                    const double bd = 0.5 * A.coeff * img_area[r] / na;
+                    rmine[r] = true;
+                    rval[r] = -bd;
+                    der0 += bd;
+                }
+                continue;
+            }
             const double ux = C.ax[r] / na, uy = C.ay[r] / na, uz = C.az[r] / na;
             const int i0 = C.F.at(0, f);
             const double x0 = C.F.X[i0], y0 = C.F.Y[i0], z0 = C.F.Z[i0];
@@ -650,7 +831,7 @@ __global__ void __launch_bounds__(64) k_cells3d(const Cell3DArgs A, const int *l
                 continue;
             }
         }
-        const int r = cell3d<FPL, MAXV>(A, s, C);
+        const int r = cell3d<FPL, MAXV>(A, s, C, A.img_backup ? A.img_backup + WB * size_t(gw) : nullptr);
         if (r == 1) {
             if (next_list) {
                 if (lane == 0) next_list[atomicAdd(next_cnt, 1)] = int(s);
@@ -699,6 +880,13 @@ constexpr long long G4_WARPS = 148 * 8;
 size_t cells3d_scratch_bytes() {
     const size_t a = warp_smem_bytes<4, 64>() * G3_WARPS, b = warp_smem_bytes<8, 128>() * G4_WARPS;
     return (a > b ? a : b) + 256;
+}
+
+size_t cells3d_image_backup_bytes() {
+    // the most warps of any pass times its face storage
+    const size_t p1 = warp_smem_bytes<1, 16>() * 148 * 7 * 2, p2 = warp_smem_bytes<2, 32>() * 148 * 3;
+    const size_t p3 = warp_smem_bytes<4, 64>() * G3_WARPS, p4 = warp_smem_bytes<8, 128>() * G4_WARPS;
+    return std::max(std::max(p1, p2), std::max(p3, p4)) + 256;
 }
 
 void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st) {

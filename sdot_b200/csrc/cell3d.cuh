@@ -25,6 +25,14 @@ struct Cell3DArgs {
     // get the ids domain_id(6 + k)
     int nplanes = 0;
     const double *planes = nullptr;
+    // piecewise-constant voxel image (ScaledImage, nb_coeffs = 1): nx x ny x nz
+    // values, x fastest, over [img_lo, img_hi]; each cell is integrated voxel
+    // by voxel (the density of a piece is the voxel's value times coeff).
+    // img_backup: per warp a copy of the faces (img_backup_bytes per warp).
+    const double *img = nullptr;
+    int img_n[3] = {0, 0, 0};
+    double img_lo[3] = {0, 0, 0}, img_hi[3] = {1, 1, 1};
+    char *img_backup = nullptr;
     // optional multilinear density factor (has_poly): coeff * (p0 + p1 x +
     // p2 y + p3 z + p4 xy + p5 xz + p6 yz + p7 xyz), absolute coordinates
     int has_poly = 0;
@@ -53,6 +61,8 @@ struct Cell3DArgs {
 // then those that overflowed again (128 faces of 64 vertices, then 256 faces
 // of 128 vertices, both in `scratch` of cells3d_scratch_bytes() bytes).
 size_t cells3d_scratch_bytes();
+// Bytes of the per-warp face copies of the voxel-image mode (all passes).
+size_t cells3d_image_backup_bytes();
 void cells3d_launch(const Cell3DArgs &a, void *scratch, cudaStream_t st);
 
 }  // namespace sdot

@@ -237,3 +237,30 @@ def test_two_boxes_3d_density(gpu_lib):
     shapes = [((0, 0, 0), (1, 1, 1), None, 1.0), ((1, 0, 0), (2, 1, 1), None, 0.5)]
     m_o, c_o, H_o = poly3d.integrate_shapes(p, shapes, poly=workloads.C4_DENSITY)
     check_vs_poly3d(g, m_o, c_o, H_o)
+
+
+# ---- 3D voxel images (ScaledImage with nb_coeffs = 1 in 3D)
+def test_voxel_image_3d(gpu_lib, ref_oracle):
+    rng = np.random.default_rng(310)
+    n = 500
+    p = rng.random((n, 3))
+    img = rng.uniform(0.5, 1.5, (6, 7, 8))  # (nz, ny, nx)
+    gpu, ref = make_pair(p, np.zeros(n), ref_oracle, image=img)
+    check_all(gpu, ref, n, rtol=1e-12, rtol_hess=1e-11)
+    assert abs(gpu.domain_measure() - ref.domain_measure()) < 1e-14
+    assert abs(gpu.integrals().sum() - img.mean()) < 1e-12
+
+
+def test_voxel_image_config4_stand_in(gpu_lib, ref_oracle):
+    # the 3D workload's density 1 + 0.3 xyz as a 32^3 voxel image holding each
+    # voxel's mean (exact for this trilinear monomial), the stand-in the
+    # reference can integrate
+    c = workloads.config4(n=20_000)
+    k = 32
+    g1 = (np.arange(k) + 0.5) / k
+    Z, Y, X = np.meshgrid(g1, g1, g1, indexing="ij")
+    img = 1 + 0.3 * X * Y * Z
+    img /= img.mean()
+    n = len(c["weights"])
+    gpu, ref = make_pair(c["positions"], c["weights"], ref_oracle, image=img)
+    check_all(gpu, ref, n, rtol=1e-12, rtol_hess=1e-11)
