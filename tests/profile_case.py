@@ -1,14 +1,16 @@
 """Evaluation CLI for profiling runs (not a test module: pytest collects
 test_*.py only).
 
-    python tests/profile_case.py CASE REPS
+    python tests/profile_case.py CASE REPS [LINEAR_SOLVER TOL]
 
 Builds one named workload and evaluates it REPS times (masses, centroids,
 Hessian), printing the stage times of each evaluation; the commands recorded
 under profiles/ run this.  CASE is c2_N (the 2D clustered mix at N Diracs),
 c3_N (the 2D image + disc-clip workload at N Diracs), c4_N (the 3D mix with
 its density) or serving_K (request K < 100 of the seeded 100-request serving
-stream, w = 0).  A suffix "_mixed" runs the mixed-precision path.
+stream, w = 0).  A suffix "_mixed" runs the mixed-precision path.  With
+LINEAR_SOLVER ("fp64" or "fp32_refined") and TOL it runs one Newton solve from
+w = 0 (the clustered case c2m_N mirrors the clusters at the box faces).
 """
 import os
 import sys
@@ -31,6 +33,12 @@ def main(argv):
     if case.startswith("c2_"):
         c = workloads.config2(n=int(case[3:]))
         p, w = c["positions"], c["weights"]
+    elif case.startswith("c2m_"):
+        n = int(case[4:])
+        rng = np.random.default_rng(workloads.SEED0 + 2)
+        p = np.concatenate([workloads.uniform_points(n // 2, 2, rng),
+                            workloads.clustered_points(n - n // 2, 2, rng, boundary="reflect")])
+        w = np.zeros(n)
     elif case.startswith("c3_"):
         c = workloads.config3(n=int(case[3:]))
         p, w, image, ball = c["positions"], c["weights"], c["image"], True
@@ -50,6 +58,14 @@ def main(argv):
         g.add_box_shape(np.zeros(dim), np.ones(dim))
     if density is not None:
         g.set_polynomial_density(density)
+    if len(argv) > 2:
+        # a Newton solve with the given linear solver ("fp64" or
+        # "fp32_refined") to the relative mass tolerance argv[3]
+        t = np.full(len(w), (0.8 if image is not None else 1.0) / len(w))
+        rep = g.solve_weights(t, rel_mass_tol=float(argv[3]), linear_solver=argv[2], raise_on_failure=False)
+        print(case, argv[2], {k: rep[k] for k in ("status", "iterations", "pcg_iterations", "max_rel_mass_error",
+                                                 "time_ms")}, flush=True)
+        return
     for k in range(reps):
         g.set_weights(w)
         g.evaluate()
