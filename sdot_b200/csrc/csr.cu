@@ -111,9 +111,8 @@ __global__ void k_unpermute(const double *in, double *out, long long n, int d, c
 // number of zero entries (empty cells), added to *count
 __global__ void k_count_zeros(const double *m, long long n, unsigned long long *count) {
     const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const bool z = s < n && m[s] == 0.0;
-    const unsigned b = __ballot_sync(0xffffffffu, z);
-    if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, (unsigned long long)__popc(b));
+    const int z = __syncthreads_count(s < n && m[s] == 0.0);  // one atomic per block
+    if (threadIdx.x == 0 && z) atomicAdd(count, (unsigned long long)z);
 }
 
 // ---- domains of several shapes: one cell pass per shape, summed here

@@ -466,6 +466,67 @@ __global__ void k_mg_post(M A, long long n, long long gauge, const double *scal,
     }
 }
 
+// The same two steps on a coarse level, four lanes per row (a warp holds the
+// eight rows of one aggregate): the coarse rows are up to MG_CAP_MAX entries
+// wide and the levels small, so one thread per row left each kernel bound by
+// the latency of a long chain of dependent loads.  Each lane sums every
+// fourth entry of its row; the partial sums are combined in a fixed order.
+constexpr int CL = 4;  // lanes per coarse row
+__global__ void k_mg_pre_coarse(EllViewT<double> A, long long n, const double *dinv, const double *r, double *z,
+                                double *rc) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, sub = lane & (CL - 1);
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long nagg = (n + MG_B - 1) / MG_B;
+    for (long long g = warp; g < nagg; g += nw) {
+        const long long i = g * MG_B + (lane >> 2);
+        // z = w D^-1 r; t = r - A z (A z from the smoothed values w D^-1 r)
+        double acc = 0, ri = 0;
+        if (i < n) {
+            ri = r[i];
+            if (sub == 0) z[i] = MG_OMEGA * dinv[i] * ri;
+            const int m = A.cnt[i];
+            for (int k = sub; k < m; k += CL) {
+                const long long c = A.col[k * A.stride + i];
+                acc += A.val[k * A.stride + i] * (MG_OMEGA * dinv[c] * r[c]);
+            }
+        }
+        acc += __shfl_xor_sync(FULL, acc, 1);
+        acc += __shfl_xor_sync(FULL, acc, 2);
+        double t = i < n && sub == 0 ? ri - acc : 0.0;
+        // the aggregate's residual: the rows in order (lanes 0, 4, ..., 28)
+        for (int o = 4; o < 32; o <<= 1) t += __shfl_xor_sync(FULL, t, o);
+        if (lane == 0) rc[g] = t;
+    }
+}
+
+__global__ void k_mg_post_coarse(EllViewT<double> A, long long n, const double *dinv, const double *r, const double *z,
+                                 const double *zc, double *zo) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, sub = lane & (CL - 1);
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long nrow = (n + 7) / 8 * 8;
+    for (long long i0 = warp * 8; i0 < nrow; i0 += nw * 8) {
+        const long long i = i0 + (lane >> 2);
+        double acc = 0;
+        if (i < n) {
+            const int m = A.cnt[i];
+            for (int k = sub; k < m; k += CL) {
+                const long long c = A.col[k * A.stride + i];
+                acc += A.val[k * A.stride + i] * (z[c] + zc[c / MG_B]);
+            }
+        }
+        acc += __shfl_xor_sync(FULL, acc, 1);
+        acc += __shfl_xor_sync(FULL, acc, 2);
+        if (i < n && sub == 0) {
+            const double zi = z[i] + zc[i / MG_B];
+            zo[i] = zi + MG_OMEGA * dinv[i] * (r[i] - acc);
+        }
+    }
+}
+
 // Dense inverse of the coarsest level (nc <= MG_COARSE rows, one block of
 // MG_COARSE threads, thread t owns row t).  Gauss-Jordan without pivoting
 // (the matrix is symmetric positive semi-definite); a pivot below 1e-13 of
@@ -657,15 +718,13 @@ void mg_vcycle(const M &A, long long gauge, const double *scal, const T *dinv0, 
     k_mg_pre<M, T, double><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].r);
     for (int l = 1; l < pl.L; ++l) {
         const MgLevelT<double> &v = pl.lev[l];
-        k_mg_pre<EllViewT<double>, double, double><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
-                                                                   pl.lev[l + 1].r);
+        k_mg_pre_coarse<<<coarse_grid(4 * v.n), TB, 0, st>>>(ell(v), v.n, v.dinv, v.r, v.z, pl.lev[l + 1].r);
     }
     const MgLevelT<double> &c = pl.lev[pl.L];
     k_mg_coarsest_apply<double><<<1, MG_COARSE, 0, st>>>(pl.cinv, int(c.n), c.r, c.zo);
     for (int l = pl.L - 1; l >= 1; --l) {
         const MgLevelT<double> &v = pl.lev[l];
-        k_mg_post<EllViewT<double>, false, double, double><<<coarse_grid(v.n), TB, 0, st>>>(ell(v), v.n, -1, scal, v.dinv, v.r, v.z,
-                                                                           pl.lev[l + 1].zo, v.zo, nullptr, nullptr);
+        k_mg_post_coarse<<<coarse_grid(4 * v.n), TB, 0, st>>>(ell(v), v.n, v.dinv, v.r, v.z, pl.lev[l + 1].zo, v.zo);
     }
     k_mg_post<M, true, T, double><<<g, TB, 0, st>>>(A, n, gauge, scal, dinv0, r0, zpre0, pl.lev[1].zo, z0, partial, p0);
 }
