@@ -139,6 +139,23 @@ int sdot_get_der_integrals_wrt_weights(sdot_ctx *ctx, int64_t *offsets, int64_t 
  * domain edge, -2 for a disc arc.  Two-phase like the Hessian.               */
 int sdot_get_neighbors(sdot_ctx *ctx, int64_t *offsets, int64_t *ids, int64_t *count_inout, int mem_space);
 
+/* get_der_centroids_and_integrals_wrt_weight_and_positions( m_offsets,
+ *   m_columns, m_values, v_values, grid, bounds, positions, weights, n, rf )
+ *   (get_der_centroids_and_integrals_wrt_weight_and_positions.h:17-216), 2D:
+ * the derivatives of (centroid x, centroid y, mass) of every cell with
+ * respect to (x, y, weight) of every Dirac, as CSR over 3 n rows and columns
+ * (row 3 i + d: output d of cell i; column 3 j + e: input e of Dirac j), and
+ * v_values[3 n] = (centroid x, centroid y, mass).  The blocks are the
+ * reference's, including its division of the centroid rows by
+ * mass + (mass == 1).  Two-phase like the Hessian (columns == NULL: *nnz_inout
+ * receives nnz).  Box / convex one-shape domains (periodic translations
+ * allowed), without the disc clip; cells of at most 64 vertices
+ * (SDOT_CAPACITY beyond).                                                    */
+int sdot_get_der_centroids_and_integrals_wrt_weight_and_positions(sdot_ctx *ctx, int64_t *offsets,
+                                                                   int64_t *columns, double *values,
+                                                                   double *v_values, int64_t *nnz_inout,
+                                                                   int mem_space);
+
 /* ---- rasterisation ----------------------------------------------------------
  * get_image_integrals( res, grid, bounds, positions, weights, n, rf, min_pt,
  *   max_pt, nbp )  (get_image_integrals.h:16-78): for the raster of

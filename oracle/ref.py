@@ -68,6 +68,8 @@ def load():
         "ref_timings": (None, [P, P]),
         "ref_get_image_integrals": (None, [P, P, P, P, P]),
         "ref_set_translations": (None, [P, P, I64]),
+        "ref_der_pos": (I64, [P]),
+        "ref_der_pos_copy": (None, [P, P, P, P, P]),
         "ref_get_image_of_cell_nums": (None, [P, P, P, P, P]),
     }
     for k, (r, a) in sig.items():
@@ -187,6 +189,22 @@ class RefPowerDiagram:
         ids = np.zeros(cnt, dtype=np.int64)
         self.L.ref_neighbors_copy(self.h, _p(off), _p(ids))
         return off, ids
+
+    def der_centroids_and_integrals_wrt_weight_and_positions(self):
+        """get_der_centroids_and_integrals_wrt_weight_and_positions: CSR over
+        (dim + 1) n rows and columns (offsets, columns, values) and the
+        values (centroid, mass) per Dirac."""
+        self._ensure()
+        nnz = self.L.ref_der_pos(self.h)
+        if nnz < 0:
+            raise RuntimeError("void cell")
+        k = self.dim + 1
+        off = np.zeros(k * self.n + 1, dtype=np.int64)
+        col = np.zeros(nnz, dtype=np.int64)
+        val = np.zeros(nnz)
+        v = np.zeros(k * self.n)
+        self.L.ref_der_pos_copy(self.h, _p(off), _p(col), _p(val), _p(v))
+        return off, col, val, v
 
     def set_translations(self, translations):
         t = _f(np.asarray(translations, dtype=np.float64).reshape(-1, self.dim))

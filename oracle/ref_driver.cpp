@@ -28,6 +28,7 @@
 #include "src/sdot/PowerDiagram/get_der_integrals_wrt_weights.h"
 #include "src/sdot/PowerDiagram/get_image_integrals.h"
 #include "src/sdot/PowerDiagram/get_image_of_cell_nums.h"
+#include "src/sdot/PowerDiagram/get_der_centroids_and_integrals_wrt_weight_and_positions.h"
 #include "src/sdot/Domains/ConvexPolyhedronAssembly.h"
 #include "src/sdot/Domains/ScaledImage.h"
 #include "src/sdot/Integration/Unit.h"
@@ -206,6 +207,21 @@ struct Ctx : CtxBase {
         return err;
     }
 
+    // get_der_centroids_and_integrals_wrt_weight_and_positions
+    // (get_der_centroids_and_integrals_wrt_weight_and_positions.h:17-216), into
+    // the der* members (offsets of (dim + 1) n rows)
+    std::vector<std::size_t> dp_offsets, dp_columns;
+    std::vector<double> dp_values, dp_v;
+    int der_pos() {
+        int err = 0;
+        with_bounds_and_rf([&](auto &bounds, auto rf) {
+            err = get_der_centroids_and_integrals_wrt_weight_and_positions(dp_offsets, dp_columns, dp_values, dp_v, grid,
+                                                                           bounds, pos.data(), w.data(), w.size(), rf,
+                                                                           false);
+        });
+        return err;
+    }
+
     // get_image_integrals (get_image_integrals.h:16-78) and
     // get_image_of_cell_nums (get_image_of_cell_nums.h:13-80), 2D
     void image_integrals(const double *lo, const double *hi, const std::int64_t *nbp, double *out, bool nums,
@@ -361,6 +377,22 @@ int ref_get_der_integrals_wrt_weights(void *h, int stop_if_void) {
     return dispatch(h, [&](auto &c) { return c.der(stop_if_void); });
 }
 std::int64_t ref_der_nnz(void *h) { return static_cast<CtxBase *>(h)->columns.size(); }
+// position derivatives (2D): computes, returns nnz; then ref_der_pos_copy
+std::int64_t ref_der_pos(void *h) {
+    return dispatch(h, [&](auto &c) -> std::int64_t {
+        if (c.der_pos()) return -1;
+        return std::int64_t(c.dp_columns.size());
+    });
+}
+void ref_der_pos_copy(void *h, std::int64_t *offsets, std::int64_t *columns, double *values, double *v) {
+    dispatch(h, [&](auto &c) {
+        for (std::size_t i = 0; i < c.dp_offsets.size(); ++i) offsets[i] = std::int64_t(c.dp_offsets[i]);
+        for (std::size_t i = 0; i < c.dp_columns.size(); ++i) columns[i] = std::int64_t(c.dp_columns[i]);
+        std::memcpy(values, c.dp_values.data(), c.dp_values.size() * sizeof(double));
+        std::memcpy(v, c.dp_v.data(), c.dp_v.size() * sizeof(double));
+        return 0;
+    });
+}
 void ref_der_copy(void *h, std::int64_t *offsets, std::int64_t *columns, double *values, double *masses) {
     CtxBase *b = static_cast<CtxBase *>(h);
     for (std::size_t i = 0; i < b->offsets.size(); ++i) offsets[i] = b->offsets[i];

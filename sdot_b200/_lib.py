@@ -96,6 +96,8 @@ SIGNATURES = {
     "sdot_get_der_integrals_wrt_weights": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int]),
     "sdot_get_neighbors": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int]),
     "sdot_get_image_integrals": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
+    "sdot_get_der_centroids_and_integrals_wrt_weight_and_positions": (ctypes.c_int, [_P, _P, _P, _P, _P, _P,
+                                                                                     ctypes.c_int]),
     "sdot_get_image_of_cell_nums": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
     "sdot_solve": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.POINTER(SdotNewtonOptions),
                                   ctypes.POINTER(SdotNewtonReport)]),

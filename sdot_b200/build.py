@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsdot_b200.so")
 SOURCES = ["prims.cu", "tree.cu", "cell2d.cu", "cell3d.cu", "csr.cu", "solve.cu", "api.cu", "server.cu", "peaks.cu",
-           "noalloc.cu"]
+           "noalloc.cu", "derpos.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

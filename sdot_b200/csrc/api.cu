@@ -3,6 +3,7 @@
 #include "cell2d.cuh"
 #include "cell3d.cuh"
 #include "csr.cuh"
+#include "derpos.cuh"
 #include "geom2d.cuh"
 #include "prims.cuh"
 #include "solve.cuh"
@@ -1639,6 +1640,77 @@ int sdot_get_image_of_cell_nums(sdot_ctx *ctx, const double *min_pt, const doubl
         ctx->rasterize(min_pt, max_pt, nb_pixels[0], nb_pixels[1], true);
         ctx->copy_out(out, ctx->ras_nums, size_t(nb_pixels[0] * nb_pixels[1]) * sizeof(int64_t), mem_space);
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return ctx->finish_status();
+    });
+}
+
+int sdot_get_der_centroids_and_integrals_wrt_weight_and_positions(sdot_ctx *ctx, int64_t *offsets,
+                                                                   int64_t *columns, double *values,
+                                                                   double *v_values, int64_t *nnz_inout,
+                                                                   int mem_space) {
+    return guarded(ctx, [&] {
+        if (!nnz_inout) throw BadArg("null nnz");
+        if (ctx->dim != 2) throw Unsupported("position derivatives are available in 2D");
+        ctx->check_domain();
+        if (ctx->ball) throw Unsupported("position derivatives with the disc clip are not available in this build");
+        if (ctx->mode != DM_SINGLE && ctx->mode != DM_PERIODIC)
+            throw Unsupported("position derivatives are available for one-shape domains");
+        ctx->evaluate_neighbors();
+        const long long n = ctx->n;
+        // block counts per Dirac, their scan, then the rows
+        ctx->reserve_stage(std::max<long long>(n + 1, 1));
+        long long *counts = ctx->cnt_orig, *boff = ctx->stage_i;
+        SDOT_CUDA(cudaMemsetAsync(ctx->err, 0, sizeof(unsigned), ctx->stream));
+        derpos_count(ctx->nb, n, ctx->tree2.pos, ctx->tree2.w, ctx->perm(), ctx->start_n, ctx->d_start, ctx->coeff,
+                     int(ctx->trans_h.size() / 2), ctx->d_trans, counts, ctx->err, ctx->stream);
+        scan_exclusive_total<long long>(counts, boff, n, ctx->scan_tmp, ctx->stream);
+        long long total = 0;
+        unsigned e = 0;
+        SDOT_CUDA(cudaMemcpyAsync(&total, boff + n, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+        SDOT_CUDA(cudaMemcpyAsync(&e, ctx->err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (e & DE_CAPACITY) {
+            ctx->last_error = "a cell has more than 64 vertices (the position derivatives' capacity)";
+            return int(SDOT_CAPACITY);
+        }
+        const long long nnz = 9 * total;
+        if (!columns) {
+            *nnz_inout = nnz;
+            return ctx->finish_status();
+        }
+        if (*nnz_inout < nnz) throw BadArg("columns/values buffers smaller than nnz");
+        if (!offsets || !values || !v_values) throw BadArg("null output");
+        long long *d_off = reinterpret_cast<long long *>(offsets), *d_col = reinterpret_cast<long long *>(columns);
+        double *d_val = values, *d_v = v_values;
+        // one-off host staging, freed on every exit
+        struct Staging {
+            long long *off = nullptr, *col = nullptr;
+            double *val = nullptr, *v = nullptr;
+            ~Staging() { dfree(off); dfree(col); dfree(val); dfree(v); }
+        } stg;
+        long long *&t_off = stg.off, *&t_col = stg.col;
+        double *&t_val = stg.val, *&t_v = stg.v;
+        if (mem_space != SDOT_DEVICE) {
+            dalloc(t_off, size_t(3 * n + 1));
+            dalloc(t_col, size_t(std::max<long long>(nnz, 1)));
+            dalloc(t_val, size_t(std::max<long long>(nnz, 1)));
+            dalloc(t_v, size_t(3 * n));
+            d_off = t_off;
+            d_col = t_col;
+            d_val = t_val;
+            d_v = t_v;
+        }
+        derpos_write(ctx->nb, n, ctx->tree2.pos, ctx->tree2.w, ctx->perm(), ctx->start_n, ctx->d_start, ctx->coeff,
+                     int(ctx->trans_h.size() / 2), ctx->d_trans, boff, d_off, d_col, d_val, d_v, ctx->stream);
+        if (mem_space != SDOT_DEVICE) {
+            SDOT_CUDA(cudaMemcpyAsync(offsets, t_off, size_t(3 * n + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(columns, t_col, size_t(nnz) * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(values, t_val, size_t(nnz) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(v_values, t_v, size_t(3 * n) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
+        *nnz_inout = nnz;
         return ctx->finish_status();
     });
 }

@@ -197,6 +197,22 @@ class PowerDiagram:
                                                  SDOT_HOST))
         return offsets, ids
 
+    def der_centroids_and_integrals_wrt_weight_and_positions(self):
+        """get_der_centroids_and_integrals_wrt_weight_and_positions (2D): CSR
+        (offsets, columns, values) over 3 n rows and columns -- row 3 i + d is
+        output d (centroid x, centroid y, mass) of cell i, column 3 j + e input
+        e (x, y, weight) of Dirac j -- and the values (3 n: centroid, mass)."""
+        fn = self._lib.sdot_get_der_centroids_and_integrals_wrt_weight_and_positions
+        nnz = ctypes.c_int64(0)
+        self._check(fn(self._ctx, None, None, None, None, ctypes.byref(nnz), SDOT_HOST))
+        n3 = 3 * self.nb_diracs
+        off = np.empty(n3 + 1, dtype=np.int64)
+        col = np.empty(nnz.value, dtype=np.int64)
+        val = np.empty(nnz.value)
+        v = np.empty(n3)
+        self._check(fn(self._ctx, _ptr(off), _ptr(col), _ptr(val), _ptr(v), ctypes.byref(nnz), SDOT_HOST))
+        return off, col, val, v
+
     def image_integrals(self, min_pt, max_pt, nb_pixels):
         """get_image_integrals: for the raster of nb_pixels = (nx, ny) pixels
         over [min_pt, max_pt], an array (ny, nx, 3) holding per pixel
