@@ -1282,7 +1282,7 @@ int sdot_add_convex_polyhedron_shape(sdot_ctx *ctx, const double *points, const 
             double d = std::sqrt(nx * nx + ny * ny) + 1e-40;
             un[2 * i] = nx / d;
             un[2 * i + 1] = ny / d;
-            nv = plane_cut(hp.view(), nv, cap, points[2 * i], points[2 * i + 1], un[2 * i], un[2 * i + 1], int(i), false);
+            nv = plane_cut(hp.view(), nv, cap, points[2 * i], points[2 * i + 1], un[2 * i], un[2 * i + 1], int(i));
             if (nv <= 0) break;
         }
         if (nv <= 0) throw BadArg("empty convex polyhedron");

@@ -462,13 +462,22 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
         // ---- the vertex pass shared by both kinds of step (bit k: vertex k
         // is outside the bisector, or fails the eviction test)
         unsigned mask = 0;
-        for (int k = 0; k < n; ++k) {
-            const double px = cell.X(k), py = cell.Y(k);
-            const double d = (ox - px) * nx + (oy - py) * ny;
-            const double qx = fmin(hi0, fmax(lo0, px)), qy = fmin(hi1, fmax(lo1, py));
-            const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
-            const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - maxw;
-            mask |= unsigned(is_cut ? d < 0.0 : !(lhs <= rhs)) << k;
+        if (is_cut) {
+            for (int k = 0; k < n; ++k) {
+                const double d = (ox - cell.X(k)) * nx + (oy - cell.Y(k)) * ny;
+                mask |= unsigned(d < 0.0) << k;
+            }
+        } else {
+            for (int k = 0; k < n; ++k) {
+                const double px = cell.X(k), py = cell.Y(k);
+                const double qx = fmin(hi0, fmax(lo0, px)), qy = fmin(hi1, fmax(lo1, py));
+                const double lhs = (c0x - px) * (c0x - px) + (c0y - py) * (c0y - py) - w0;
+                const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - maxw;
+                if (!(lhs <= rhs)) {  // this vertex fails: the box is needed
+                    mask = 1u;
+                    break;
+                }
+            }
         }
         const CutFacts f = cut_facts(mask, n);
         SDOT_WORK_ADD(is_cut ? 0 : 2, 1);
@@ -476,7 +485,7 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
         if (is_cut) {
             if (f.nb_out) {
                 SDOT_WORK_ADD(4, 1);
-                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, PER ? j + (sym + 1) * int(A.n) : j, true, f);
+                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, PER ? j + (sym + 1) * int(A.n) : j, f);
                 if (n <= 0) return n;
             }
             j = jn;
@@ -498,14 +507,15 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             }
             float key[4];
             int ch[4];
+            int nk = 0;
             for (int c = 0; c < nch; ++c) {
                 const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
                 const double mx = c0x - tr(0.5 * (cn.lo[0] + cn.hi[0]), tx);
                 const double my = c0y - tr(0.5 * (cn.lo[1] + cn.hi[1]), ty);
-                key[c] = float(mx * mx + my * my);
-                ch[c] = first + c;
+                key[nk] = float(mx * mx + my * my);
+                ch[nk++] = first + c;
             }
-            for (int i = 1; i < nch; ++i) {  // farthest first
+            for (int i = 1; i < nk; ++i) {  // farthest first
                 const float kk = key[i];
                 const int cc = ch[i];
                 int q = i - 1;
@@ -517,7 +527,7 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 key[q + 1] = kk;
                 ch[q + 1] = cc;
             }
-            for (int c = 0; c < nch; ++c) {
+            for (int c = 0; c < nk; ++c) {
                 if (has_top) stack[sp++] = top;
                 top = ch[c];
                 has_top = true;
@@ -587,7 +597,7 @@ SDOT_KFN int build_cell_f32(const Cell2DArgs &A, long long s, const PolyView<flo
             const double p0x = A.start_xy[2 * e] - c0x, p0y = A.start_xy[2 * e + 1] - c0y;
             const double dx = A.start_xy[2 * e1] - A.start_xy[2 * e];
             const double dy = A.start_xy[2 * e1 + 1] - A.start_xy[2 * e + 1];
-            n = plane_cut(cell, n, cap, float(p0x), float(p0y), float(dy), float(-dx), domain_id(e), true);
+            n = plane_cut(cell, n, cap, float(p0x), float(p0y), float(dy), float(-dx), domain_id(e));
         }
         if (n <= 0) return -4;  // the square misses the domain
     } else {
@@ -668,7 +678,7 @@ SDOT_KFN int build_cell_f32(const Cell2DArgs &A, long long s, const PolyView<flo
         if (is_cut) {
             if (f.nb_out) {
                 if (f.nb_out == n && has_local()) return -4;  // empty within the square only
-                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, true, f);
+                n = plane_cut_apply(cell, n, cap, ox, oy, nx, ny, j, f);
                 if (n <= 0) return n;
             }
             ++j;

@@ -45,9 +45,9 @@ struct PolyView {
 };
 
 // Cut the polygon (n vertices, capacity cap) by the half-plane
-// {p : (o - p) . nrm >= 0}; the new edge gets `cut_id`.  When `normalize` is
-// set the distances (and so the interpolation ratios) are divided by |nrm|
-// as the reference does for un-normalised normals (N<0>).
+// {p : (o - p) . nrm >= 0}; the new edge gets `cut_id`.  The reference
+// divides its distances by |nrm| for un-normalised normals (N<0>); the
+// interpolation ratios are the same without it.
 // Returns the new vertex count, or -1 if the result would exceed `cap`.
 // The facts the reference reads from its `outside` bitset: count, first set
 // bit, first clear bit, bits 1 and n - 1 (one pass over the vertices).
@@ -84,30 +84,44 @@ SDOT_HD CutFacts cut_facts(unsigned mask, int n) {
 }
 
 template <class T>
-SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize,
+SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id,
                             const CutFacts &f);
 
 template <class T>
-SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize) {
+SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id) {
     CutFacts f;
     for (int k = 0; k < n; ++k) {
         const T d = (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny;
         f.add(k, n, d < T(0));
     }
-    return plane_cut_apply(p, n, cap, ox, oy, nx, ny, cut_id, normalize, f);
+    return plane_cut_apply(p, n, cap, ox, oy, nx, ny, cut_id, f);
 }
 
-// The cut itself, given the classification of the vertices.
+// The cut itself, given the classification of the vertices.  The new
+// vertices sit at the ratios s_a / (s_b - s_a) of the signed distances along
+// their edges; the ratios do not depend on the scale of the normal, so the
+// distances are left unnormalised, and in FP64 both ratios come from one division (1 / (u v), u and v the two
+// distance differences: products of coordinates, far from underflow).
 template <class T>
-SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id, bool normalize,
+SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id,
                             const CutFacts &f) {
     const int nb_out = f.nb_out, first_out = f.first_out, first_in = f.first_in;
     const bool out1 = f.out1, out_last = f.out_last;
     if (nb_out == 0) return n;
     if (nb_out == n) return 0;
-    T inv = T(1);
-    if (normalize) inv = T(1) / sqrt(nx * nx + ny * ny);
-    auto dist = [&](int k) -> T { return ((ox - p.X(k)) * nx + (oy - p.Y(k)) * ny) * inv; };
+    auto dist = [&](int k) -> T { return (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny; };
+    // the two edge ratios a / (b - a), c / (d - c)
+    auto ratios = [](T a, T b, T c, T d, T &m1, T &m2) {
+        const T u = b - a, v = d - c;
+        if constexpr (sizeof(T) == 8) {
+            const T r = T(1) / (u * v);
+            m1 = a * v * r;
+            m2 = c * u * r;
+        } else {  // FP32: u v of small cells can underflow
+            m1 = a / u;
+            m2 = c / v;
+        }
+    };
 
     int i1 = first_out;
     if (nb_out == 1) {
@@ -115,8 +129,8 @@ SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T 
         int i0 = (i1 + n - 1) % n, i2 = (i1 + 1) % n;
         T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1), p2x = p.X(i2), p2y = p.Y(i2);
         T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2);
-        T m0 = s0 / (s1 - s0);
-        T m1 = s2 / (s1 - s2);
+        T m0, m1;
+        ratios(s0, s1, s2, s1, m0, m1);
         for (int i = n; i > i1 + 1; --i) p.copy(i, i - 1);
         p.X(i1 + 1) = p2x - m1 * (p1x - p2x);
         p.Y(i1 + 1) = p2y - m1 * (p1y - p2y);
@@ -132,8 +146,8 @@ SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T 
         T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
         T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
         T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1 = s0 / (s1 - s0);
-        T m2 = s3 / (s2 - s3);
+        T m1, m2;
+        ratios(s0, s1, s3, s2, m1, m2);
         p.X(i1) = p0x - m1 * (p1x - p0x);
         p.Y(i1) = p0y - m1 * (p1y - p0y);
         p.I(i1) = cut_id;
@@ -150,8 +164,8 @@ SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T 
         T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
         T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
         T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1 = s0 / (s1 - s0);
-        T m2 = s3 / (s2 - s3);
+        T m1, m2;
+        ratios(s0, s1, s3, s2, m1, m2);
         int id2 = p.I(i2);
         p.X(0) = p3x - m2 * (p2x - p3x);
         p.Y(0) = p3y - m2 * (p2y - p3y);
@@ -168,8 +182,8 @@ SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T 
         T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
         T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
         T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1 = s0 / (s1 - s0);
-        T m2 = s3 / (s2 - s3);
+        T m1, m2;
+        ratios(s0, s1, s3, s2, m1, m2);
         int id2 = p.I(i2);
         p.X(i1) = p0x - m1 * (p1x - p0x);
         p.Y(i1) = p0y - m1 * (p1y - p0y);
