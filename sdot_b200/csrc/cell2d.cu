@@ -1290,6 +1290,10 @@ void launch_all(const Cell2DArgs &a, void *scratch, cudaStream_t st) {
                                        int(fast_smem<MODE, BALL>(T2D_MAX, false))));
         SDOT_CUDA(cudaFuncSetAttribute(k_cells2d_mixed<MODE, BALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(fast_smem<MODE, BALL>(T2D_MAX, true))));
+        // 72% of the shared memory capacity (164 KB: 16 warps of 64-thread
+        // blocks) leaves the rest to L1 for the walk's tree, Diracs and stack;
+        // measured 2% faster on the 1M clustered mix than the largest carveout
+        SDOT_CUDA(cudaFuncSetAttribute(k_cells2d<MODE, BALL>, cudaFuncAttributePreferredSharedMemoryCarveout, 72));
     });
     if (a.start_n > CAP_FAST_2D) {
         // the starting polygon alone overflows the fast tier: every cell is
