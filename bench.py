@@ -105,6 +105,25 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x, device="cpu"):
+    """The largest of a per-rank float over every rank of the process group
+    (x itself without one): step times are reported as the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_per_rank, world, seconds):
+    """Whole-job cells/s of `world` independent problems of n_per_rank cells
+    each, finished in `seconds` (the slowest rank's time)."""
+    return world * n_per_rank / seconds
+
+
 def workload(n, rank, config="c2"):
     from sdot_b200 import workloads
 
@@ -336,13 +355,10 @@ def run_ours(args):
     L.sdot_kernel_launches(ctypes.byref(launches1))
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    ms = float(np.mean(step_ms))
+    ms = max_over_ranks(float(np.mean(step_ms)), dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * n / (ms * 1e-3)
+    value = replica_value(n, world, ms * 1e-3)
 
     # ---- e2e: public ABI from pinned host buffers (copies included)
     off_h = torch.empty(n + 1, dtype=torch.int64).pin_memory()
@@ -379,11 +395,7 @@ def run_ours(args):
         step_e2e()
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(e2e_times))
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(np.mean(e2e_times)), dev)
     h2d = n * dim * 8 + n * 8
     d2h = n * dim * 8 + n * 8 + (n + 1) * 8 + nnz.value * 16 + n * 8
 
@@ -416,7 +428,7 @@ def run_ours(args):
            "config": {"workload": wl, "n_diracs_per_gpu": n, "precision": args.precision,
                       "parallelism": f"weak x{world} (independent problem per GPU)",
                       "l2": "flushed between steps (256 MB write)"},
-           "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "e2e": {"value": replica_value(n, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "gpu_launches": int(launches1.value - launches0.value),
            "roofline": roofline, "clocks": clk, "wall_timed_s": wall,
            "stages_ms": {"cells": cell}}
