@@ -100,13 +100,14 @@ SDOT_HD int plane_cut(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T 
 // The cut itself, given the classification of the vertices.  The new
 // vertices sit at the ratios s_a / (s_b - s_a) of the signed distances along
 // their edges; the ratios do not depend on the scale of the normal, so the
-// distances are left unnormalised, and in FP64 both ratios come from one division (1 / (u v), u and v the two
-// distance differences: products of coordinates, far from underflow).
+// distances are left unnormalised, and in FP64 both ratios come from one
+// division (1 / (u v), u and v the two distance differences: products of
+// coordinates, far from underflow).
 template <class T>
 SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T nx, T ny, int cut_id,
                             const CutFacts &f) {
     const int nb_out = f.nb_out, first_out = f.first_out, first_in = f.first_in;
-    const bool out1 = f.out1, out_last = f.out_last;
+    const bool out_last = f.out_last;
     if (nb_out == 0) return n;
     if (nb_out == n) return 0;
     auto dist = [&](int k) -> T { return (ox - p.X(k)) * nx + (oy - p.Y(k)) * ny; };
@@ -123,78 +124,51 @@ SDOT_HD int plane_cut_apply(const PolyView<T> &p, int n, int cap, T ox, T oy, T 
         }
     };
 
-    int i1 = first_out;
-    if (nb_out == 1) {
-        if (n + 1 > cap) return -1;
-        int i0 = (i1 + n - 1) % n, i2 = (i1 + 1) % n;
-        T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1), p2x = p.X(i2), p2y = p.Y(i2);
-        T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2);
-        T m0, m1;
-        ratios(s0, s1, s2, s1, m0, m1);
-        for (int i = n; i > i1 + 1; --i) p.copy(i, i - 1);
-        p.X(i1 + 1) = p2x - m1 * (p1x - p2x);
-        p.Y(i1 + 1) = p2y - m1 * (p1y - p2y);
-        p.I(i1 + 1) = p.I(i1);
-        p.X(i1) = p0x - m0 * (p1x - p0x);
-        p.Y(i1) = p0y - m0 * (p1y - p0y);
-        p.I(i1) = cut_id;
-        return n + 1;
-    }
-    if (nb_out == 2) {
-        if (i1 == 0 && !out1) i1 = n - 1;
-        int i0 = (i1 + n - 1) % n, i2 = (i1 + 1) % n, i3 = (i1 + 2) % n;
-        T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
-        T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
-        T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1, m2;
-        ratios(s0, s1, s3, s2, m1, m2);
-        p.X(i1) = p0x - m1 * (p1x - p0x);
-        p.Y(i1) = p0y - m1 * (p1y - p0y);
-        p.I(i1) = cut_id;
-        p.X(i2) = p3x - m2 * (p2x - p3x);
-        p.Y(i2) = p3y - m2 * (p2y - p3y);
-        return n;
-    }
-    if (i1 == 0 && out_last) {
-        // the removed run wraps over vertex 0: the polygon is rotated
-        const int nb_in = n - nb_out;
-        const int i3 = first_in;
-        i1 = nb_in + i3;
-        const int i0 = i1 - 1, i2 = i3 - 1;
-        T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
-        T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
-        T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1, m2;
-        ratios(s0, s1, s3, s2, m1, m2);
-        int id2 = p.I(i2);
-        p.X(0) = p3x - m2 * (p2x - p3x);
-        p.Y(0) = p3y - m2 * (p2y - p3y);
+    // One layout for every case.  The removed run is [i1, i2] (cyclic), the
+    // kept run [i3, i0]; A (on edge i0 -> i1) takes the cut's id, B (on edge
+    // i2 -> i3) the id of that edge.  Without wrap (the run does not hold
+    // both vertex n - 1 and vertex 0): A at i1, B at i1 + 1, the kept tail
+    // [i3, n) shifted by 2 - nb_out.  With wrap: B at 0, the kept run moved
+    // to [1, nb_in], A after it.  These are the positions of the reference's
+    // four cases (one vertex out, two, a wrapping run, a longer run).
+    const int nb_in = n - nb_out;
+    if (nb_out == 1 && n + 1 > cap) return -1;
+    const bool wrap = out_last && first_out == 0;  // nb_out >= 2 here, as nb_out == 1 cannot be both
+    const int i3 = wrap ? first_in : first_out + nb_out;  // may be n: vertex 0
+    const int i1 = wrap ? first_in + nb_in : first_out;
+    const int i0 = i1 == 0 ? n - 1 : i1 - 1;
+    const int i2 = i3 == 0 ? n - 1 : i3 - 1;
+    const int i3c = i3 == n ? 0 : i3;
+    T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
+    T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3c), p3y = p.Y(i3c);
+    T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3c);
+    T m1, m2;
+    ratios(s0, s1, s3, s2, m1, m2);
+    const T ax = p0x - m1 * (p1x - p0x), ay = p0y - m1 * (p1y - p0y);
+    const T bx = p3x - m2 * (p2x - p3x), by = p3y - m2 * (p2y - p3y);
+    const int id2 = p.I(i2);
+    if (wrap) {
+        for (int k = 0; k < nb_in; ++k) p.copy(1 + k, i3 + k);
+        p.X(0) = bx;
+        p.Y(0) = by;
         p.I(0) = id2;
-        int o = 1;
-        for (; o <= nb_in; ++o) p.copy(o, i2 + o);
-        p.X(o) = p0x - m1 * (p1x - p0x);
-        p.Y(o) = p0y - m1 * (p1y - p0y);
-        p.I(o) = cut_id;
-        return nb_in + 2;
-    }
-    {
-        int i0 = (i1 + n - 1) % n, i2 = (i1 + nb_out - 1) % n, i3 = (i1 + nb_out) % n;
-        T p0x = p.X(i0), p0y = p.Y(i0), p1x = p.X(i1), p1y = p.Y(i1);
-        T p2x = p.X(i2), p2y = p.Y(i2), p3x = p.X(i3), p3y = p.Y(i3);
-        T s0 = dist(i0), s1 = dist(i1), s2 = dist(i2), s3 = dist(i3);
-        T m1, m2;
-        ratios(s0, s1, s3, s2, m1, m2);
-        int id2 = p.I(i2);
-        p.X(i1) = p0x - m1 * (p1x - p0x);
-        p.Y(i1) = p0y - m1 * (p1y - p0y);
+        p.X(nb_in + 1) = ax;
+        p.Y(nb_in + 1) = ay;
+        p.I(nb_in + 1) = cut_id;
+    } else {
+        if (nb_out == 1) {
+            for (int i = n - 1; i >= i3; --i) p.copy(i + 1, i);
+        } else {
+            for (int i = i3; i < n; ++i) p.copy(i + 2 - nb_out, i);
+        }
+        p.X(i1) = ax;
+        p.Y(i1) = ay;
         p.I(i1) = cut_id;
-        p.X(i1 + 1) = p3x - m2 * (p2x - p3x);
-        p.Y(i1 + 1) = p3y - m2 * (p2y - p3y);
+        p.X(i1 + 1) = bx;
+        p.Y(i1 + 1) = by;
         p.I(i1 + 1) = id2;
-        const int nb_rem = nb_out - 2;
-        for (int i = i2 + 1; i < n; ++i) p.copy(i - nb_rem, i);
-        return n - nb_rem;
     }
+    return nb_in + 2;
 }
 
 #ifdef __CUDACC__
