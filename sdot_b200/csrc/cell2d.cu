@@ -367,6 +367,43 @@ SDOT_HDI void stream_cell(const P &cell, int n, Stage &st) {
     st.finish();
 }
 
+// The children [first, first + nch) of a box (2 <= nch <= 4) in ch[0 ..
+// nch), farthest first by the float squared distance from c0 to their box
+// centres (the key of the reference's queue), the box shifted by (tx, ty)
+// when PER.  A fixed network of five exchanges over four slots (missing
+// children keyed -1, after every real key) keeps the arrays in registers.
+template <bool PER>
+SDOT_HDI void order_children(const Cell2DArgs &A, int first, int nch, double c0x, double c0y, double tx, double ty,
+                             int ch[4]) {
+    float key[4] = {-1.f, -1.f, -1.f, -1.f};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        ch[c] = first + c;
+        if (c < nch) {
+            const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
+            const double cx = 0.5 * (cn.lo[0] + cn.hi[0]), cy = 0.5 * (cn.lo[1] + cn.hi[1]);
+            const double mx = c0x - (PER ? cx + tx : cx);
+            const double my = c0y - (PER ? cy + ty : cy);
+            key[c] = float(mx * mx + my * my);
+        }
+    }
+    auto cx = [&](int a, int b) {
+        if (key[a] < key[b]) {
+            const float tk = key[a];
+            key[a] = key[b];
+            key[b] = tk;
+            const int tc = ch[a];
+            ch[a] = ch[b];
+            ch[b] = tc;
+        }
+    };
+    cx(0, 1);
+    cx(2, 3);
+    cx(0, 2);
+    cx(1, 3);
+    cx(1, 2);
+}
+
 // Builds the Laguerre cell of sorted Dirac s (before any disc clipping) as a
 // machine of uniform steps, so that the 32 cells of a warp advance together.
 // The walk is SpZGrid::for_each_laguerre_cell's (SpZGrid.tcc:494-719): boxes
@@ -505,32 +542,15 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 flag_error(A.err, DE_STACK);
                 return -1;
             }
-            float key[4];
             int ch[4];
-            int nk = 0;
-            for (int c = 0; c < nch; ++c) {
-                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
-                const double mx = c0x - tr(0.5 * (cn.lo[0] + cn.hi[0]), tx);
-                const double my = c0y - tr(0.5 * (cn.lo[1] + cn.hi[1]), ty);
-                key[nk] = float(mx * mx + my * my);
-                ch[nk++] = first + c;
-            }
-            for (int i = 1; i < nk; ++i) {  // farthest first
-                const float kk = key[i];
-                const int cc = ch[i];
-                int q = i - 1;
-                while (q >= 0 && key[q] < kk) {
-                    key[q + 1] = key[q];
-                    ch[q + 1] = ch[q];
-                    --q;
+            order_children<PER>(A, first, nch, c0x, c0y, tx, ty, ch);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (c < nch) {
+                    if (has_top) stack[sp++] = top;
+                    top = ch[c];
+                    has_top = true;
                 }
-                key[q + 1] = kk;
-                ch[q + 1] = cc;
-            }
-            for (int c = 0; c < nk; ++c) {
-                if (has_top) stack[sp++] = top;
-                top = ch[c];
-                has_top = true;
             }
         } else {
             if (nd_a < 0 || nd_b > A.n) {
@@ -695,28 +715,11 @@ SDOT_KFN int build_cell_f32(const Cell2DArgs &A, long long s, const PolyView<flo
                 flag_error(A.err, DE_STACK);
                 return -1;
             }
-            float key[4];
             int ch[4];
-            for (int c = 0; c < nch; ++c) {
-                const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
-                const double mx = c0x - 0.5 * (cn.lo[0] + cn.hi[0]);
-                const double my = c0y - 0.5 * (cn.lo[1] + cn.hi[1]);
-                key[c] = float(mx * mx + my * my);
-                ch[c] = first + c;
-            }
-            for (int i = 1; i < nch; ++i) {
-                const float kk = key[i];
-                const int cc = ch[i];
-                int q = i - 1;
-                while (q >= 0 && key[q] < kk) {
-                    key[q + 1] = key[q];
-                    ch[q + 1] = ch[q];
-                    --q;
-                }
-                key[q + 1] = kk;
-                ch[q + 1] = cc;
-            }
-            for (int c = 0; c < nch; ++c) stack[sp++] = ch[c];
+            order_children<false>(A, first, nch, c0x, c0y, 0.0, 0.0, ch);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (c < nch) stack[sp++] = ch[c];
         } else {
             if (nd_a < 0 || nd_b > A.n) {
                 guard_fail(A, 2, s, node);
@@ -1163,30 +1166,13 @@ __device__ int build_cell_coop(const Cell2DArgs &A, long long s, const PolyView<
                     if (lane == 0) flag_error(A.err, DE_STACK);
                     return -1;
                 }
-                float key[4];
                 int ch[4];
-                for (int c = 0; c < nch; ++c) {
-                    const TreeNode<2> &cn = A.nodes[SDOT_CHECK_IDX(first + c, A.max_nodes, 5)];
-                    const double cx = 0.5 * (cn.lo[0] + cn.hi[0]), cy = 0.5 * (cn.lo[1] + cn.hi[1]);
-                    const double mx = c0x - (PER ? cx + tx : cx);
-                    const double my = c0y - (PER ? cy + ty : cy);
-                    key[c] = float(mx * mx + my * my);
-                    ch[c] = first + c;
+                order_children<PER>(A, first, nch, c0x, c0y, tx, ty, ch);
+                if (lane == 0) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (c < nch) wstack[sp + c] = ch[c];
                 }
-                for (int i = 1; i < nch; ++i) {  // farthest first
-                    const float kk = key[i];
-                    const int cc = ch[i];
-                    int j = i - 1;
-                    while (j >= 0 && key[j] < kk) {
-                        key[j + 1] = key[j];
-                        ch[j + 1] = ch[j];
-                        --j;
-                    }
-                    key[j + 1] = kk;
-                    ch[j + 1] = cc;
-                }
-                if (lane == 0)
-                    for (int c = 0; c < nch; ++c) wstack[sp + c] = ch[c];
                 __syncwarp();
                 sp += nch;
             } else {
