@@ -70,21 +70,30 @@ __device__ inline double shfl(double v, int src) { return __shfl_sync(FULL, v, s
 
 // Outcome of a cut: 0 done, 1 a capacity was exceeded, 2 degenerate geometry.
 template <int FPL, int MAXV>
-__device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double qb, int qid) {
+__device__ __forceinline__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double qb, int qid) {
     const int lane = threadIdx.x & 31;
     auto &F = C.F;
     auto outside = [&](int v, int f) {
         const int i = F.at(v, f);
         return qb - (qx * F.X[i] + qy * F.Y[i] + qz * F.Z[i]) < 0.0;
     };
+    // faces of at most 32 vertices keep the classification as a bit mask
+    constexpr bool MASKED = MAXV <= 32;
     int nouts[FPL];
+    unsigned om[FPL];
     bool has = false;
 #pragma unroll
     for (int r = 0; r < FPL; ++r) {
         const int f = lane + 32 * r;
         int c = 0;
-        for (int v = 0; v < C.nv[r]; ++v) c += outside(v, f);
+        unsigned mk = 0;
+        for (int v = 0; v < C.nv[r]; ++v) {
+            const bool o = outside(v, f);
+            c += o;
+            if (MASKED) mk |= unsigned(o) << v;
+        }
         nouts[r] = c;
+        om[r] = mk;
         has |= c != 0;
     }
     if (!__any_sync(FULL, has)) return 0;
@@ -109,15 +118,27 @@ __device__ int cut3(Cell3<FPL, MAXV> &C, double qx, double qy, double qz, double
         // the outside run: o1 its first vertex (predecessor inside), o2 its
         // last (successor inside); one run only, else the face is cut twice
         int o1 = -1, o2 = -1, runs = 0;
-        bool prev = outside(n - 1, f);
-        for (int v = 0; v < n; ++v) {
-            const bool o = outside(v, f);
-            if (o && !prev) {
-                o1 = v;
-                ++runs;
+        if (MASKED) {
+            // run starts: outside with the previous vertex inside; ends:
+            // outside with the next vertex inside (cyclic over n bits)
+            const unsigned mk = om[r], valid = n >= 32 ? ~0u : (1u << n) - 1u;
+            const unsigned prevm = ((mk << 1) | (mk >> (n - 1))) & valid;
+            const unsigned nextm = ((mk >> 1) | ((mk & 1u) << (n - 1))) & valid;
+            const unsigned starts = mk & ~prevm, ends = mk & ~nextm;
+            runs = __popc(starts);
+            o1 = __ffs(int(starts)) - 1;
+            o2 = __ffs(int(ends)) - 1;
+        } else {
+            bool prev = outside(n - 1, f);
+            for (int v = 0; v < n; ++v) {
+                const bool o = outside(v, f);
+                if (o && !prev) {
+                    o1 = v;
+                    ++runs;
+                }
+                if (!o && prev) o2 = v == 0 ? n - 1 : v - 1;
+                prev = o;
             }
-            if (!o && prev) o2 = v == 0 ? n - 1 : v - 1;
-            prev = o;
         }
         if (runs != 1 || o1 < 0 || o2 < 0) {
             bad = true;
@@ -297,7 +318,7 @@ struct PolyRel {
 
 // The domain box as six faces (slots 0..5), relative to c0.
 template <int FPL, int MAXV>
-__device__ void init_box(Cell3<FPL, MAXV> &C, const Cell3DArgs &A, double c0x, double c0y, double c0z) {
+__device__ __forceinline__ void init_box(Cell3<FPL, MAXV> &C, const Cell3DArgs &A, double c0x, double c0y, double c0z) {
     const int lane = threadIdx.x & 31;
     const double lo[3] = {A.box_lo[0] - c0x, A.box_lo[1] - c0y, A.box_lo[2] - c0z};
     const double hi[3] = {A.box_hi[0] - c0x, A.box_hi[1] - c0y, A.box_hi[2] - c0z};
@@ -339,7 +360,7 @@ __device__ void init_box(Cell3<FPL, MAXV> &C, const Cell3DArgs &A, double c0x, d
 // lane writes entry pos[r] when mine[r]), then the diagonal from lane 0 when
 // with_diag, into the ELL slots or, for a long row, the side buffer.
 template <int FPL>
-__device__ bool write_row(const Rows &R, long long s, int cnt, const int *pos, const bool *mine, const int *col,
+__device__ __forceinline__ bool write_row(const Rows &R, long long s, int cnt, const int *pos, const bool *mine, const int *col,
                           const double *val, bool with_diag, int diag_col, double diag_val) {
     const int lane = threadIdx.x & 31;
     long long off = 0;
@@ -382,7 +403,7 @@ __device__ void guard_fail3(const Cell3DArgs &A, int code, long long s, long lon
 // faces of C, the pyramids of apex c0 over the faces (this lane's slots only;
 // the caller sums over the warp).  Constant density.
 template <int FPL, int MAXV>
-__device__ void face_volumes(const Cell3<FPL, MAXV> &C, double &vol, double &mx, double &my, double &mz,
+__device__ __forceinline__ void face_volumes(const Cell3<FPL, MAXV> &C, double &vol, double &mx, double &my, double &mz,
                              double *area_r) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -428,7 +449,7 @@ __device__ void face_volumes(const Cell3<FPL, MAXV> &C, double &vol, double &mx,
 // (this lane's slots) into vol, m*, and per slot the value-weighted area of
 // the Dirac faces.  Returns 0, or 1 / 2 as cut3 (capacity, degenerate).
 template <int FPL, int MAXV>
-__device__ int voxel_integrals(const Cell3DArgs &A, Cell3<FPL, MAXV> &C, char *backup, double c0x, double c0y,
+__device__ __forceinline__ int voxel_integrals(const Cell3DArgs &A, Cell3<FPL, MAXV> &C, char *backup, double c0x, double c0y,
                                double c0z, double &vol, double &mx, double &my, double &mz, double *wa_r) {
     const int lane = threadIdx.x & 31;
     Faces<FPL, MAXV> B;
@@ -548,7 +569,7 @@ __device__ int voxel_integrals(const Cell3DArgs &A, Cell3<FPL, MAXV> &C, char *b
 // written), 1 (a capacity was exceeded: retry in the large pass), 2 (failed:
 // outputs written as NaN / empty row, error flagged).
 template <int FPL, int MAXV>
-__device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C, char *backup) {
+__device__ __forceinline__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C, char *backup) {
     const int lane = threadIdx.x & 31;
     const double c0x = A.pos[3 * s], c0y = A.pos[3 * s + 1], c0z = A.pos[3 * s + 2], w0 = A.w[s];
     init_box(C, A, c0x, c0y, c0z);
@@ -604,8 +625,9 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C, cha
                 status = 2;
                 break;
             }
-            // children sorted farthest first (nearest popped first); lane c
-            // keys child c, lane 0 sorts and pushes
+            // children farthest first (nearest popped first): lane c keys child
+            // c and writes it at its rank among the keys (larger keys first,
+            // equal keys in child order, as a stable sort would place them)
             float key = 0;
             if (lane < nch) {
                 const TreeNode<3> &cn = A.nodes[first + lane];
@@ -613,26 +635,13 @@ __device__ int cell3d(const Cell3DArgs &A, long long s, Cell3<FPL, MAXV> &C, cha
                              mz = 0.5 * (cn.lo[2] + cn.hi[2]) - c0z;
                 key = float(mx * mx + my * my + mz * mz);
             }
-            float keys[8];
+            int rank = 0;
 #pragma unroll
-            for (int c = 0; c < 8; ++c) keys[c] = __shfl_sync(FULL, key, c);
-            if (lane == 0) {
-                int ch[8];
-                for (int c = 0; c < nch; ++c) ch[c] = first + c;
-                for (int i = 1; i < nch; ++i) {
-                    const float kk = keys[i];
-                    const int cc = ch[i];
-                    int q = i - 1;
-                    while (q >= 0 && keys[q] < kk) {
-                        keys[q + 1] = keys[q];
-                        ch[q + 1] = ch[q];
-                        --q;
-                    }
-                    keys[q + 1] = kk;
-                    ch[q + 1] = cc;
-                }
-                for (int c = 0; c < nch; ++c) C.stack[sp + c] = ch[c];
+            for (int c = 0; c < 8; ++c) {
+                const float kc = __shfl_sync(FULL, key, c);
+                rank += c < nch && (kc > key || (kc == key && c < lane));
             }
+            if (lane < nch) C.stack[sp + rank] = first + lane;
             __syncwarp();
             sp += nch;
         } else {
