@@ -439,6 +439,50 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
     // position and weight of the next Dirac of a leaf are loaded while the
     // current one cuts.
     int stack[STACK];
+    int sp = 0;                 // stack entries below `top`
+    int top = 0;                // the node the next node step pops
+    bool has_top = true;
+    int j = 0, je = 0;          // Diracs of the current leaf still to cut by
+    double cjx = 0, cjy = 0, cjw = 0;  // Dirac j
+    int visits = 0;
+    int sym = -1;               // PER: the translation of the current walk (-1: none)
+    double tx = 0, ty = 0;      // and its vector
+    auto skip_self = [&](int k) { return (!PER || sym < 0) && k == s ? k + 1 : k; };
+    // shifted by the current translation (PER only: adding a zero would not
+    // be free, it turns -0 into +0)
+    auto tr = [&](double v, double t) { return PER ? v + t : v; };
+    while (true) {
+        // ---- the step: one cut (j < je) or one node test
+        if (PER && j >= je && !has_top && sym + 1 < A.ntrans) {
+            // the next translation's walk starts from the root again
+            ++sym;
+            tx = A.trans[2 * sym];
+            ty = A.trans[2 * sym + 1];
+            top = 0;
+            has_top = true;
+        }
+        const bool is_cut = j < je;
+        double ox = 0, oy = 0, nx = 0, ny = 0;
+        double lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0, maxw = 0;
+        int node = -1, nd_a = 0, nd_b = 0;
+        int jn = 0;
+        double njx = 0, njy = 0, njw = 0;
+        if (is_cut) {
+            bisector(c0x, c0y, w0, cjx, cjy, cjw, ox, oy, nx, ny);
+            jn = skip_self(j + 1);
+            if (jn < je) {
+                (void)SDOT_CHECK_IDX(jn, A.n, 6);
+                njx = tr(A.pos[2 * jn], tx);
+                njy = tr(A.pos[2 * jn + 1], ty);
+                njw = A.w[jn];
+            }
+        } else {
+            if (!has_top) break;
+            if (++visits > (PER ? (A.ntrans + 1) * A.max_nodes : A.max_nodes)) {  // each tree walk visits a node once
+                flag_error(A.err, DE_ITER);
+                return -1;
+            }
+            node = top;
             if (sp > 0)
                 top = stack[--sp];
             else
