@@ -18,10 +18,12 @@ enum DomainMode : int { DM_SINGLE = 0, DM_MULTI = 1, DM_IMAGE = 2, DM_IMAGE6 = 3
 // overflow it are rebuilt by the warp tier (one warp per cell, polygon in
 // global scratch).  Beyond the warp tier's capacity the call reports
 // ST_CAPACITY.
-// 14 fast vertices (280 B of shared memory per cell) let an SM hold six
-// blocks of 128 threads (the fast kernel's register cap matches): 24 warps
-// instead of 20 with 16 vertices, 4% faster on the 1M clustered mix.
-constexpr int CAP_FAST_2D = 14;
+// 13 fast vertices (260 B of shared memory per cell): with the fast
+// kernel's shared-memory carveout an SM holds more warps than with 14 or 16,
+// and the few cells of 14 or more vertices on the 1M clustered mix cost less
+// in the warp tier than the smaller occupancy would (measured: 13 vertices
+// 4.13 ms, 12: 4.16, 14: 4.23, 16: 4.54).
+constexpr int CAP_FAST_2D = 13;
 static_assert(CAP_FAST_2D <= 32, "the fast tier keeps one bit per vertex in a 32-bit mask");
 constexpr int CAP_HUGE_2D = 1024;
 // Hessian rows and neighbour lists are stored slot-major (ELL) with these
