@@ -1024,7 +1024,9 @@ __global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d(const Cell2DArgs A) {
 // whose FP32 decisions were too close to call, whose topology does not
 // re-clip cleanly, or that overflow the capacity go to the FP64 warp tier.
 template <int MODE, bool BALL>
-__global__ void __launch_bounds__(T2D_MAX) k_cells2d_mixed(const Cell2DArgs A) {
+// six blocks of T2D_MAX threads per SM, as the FP64 kernel (4% faster on the
+// 1M clustered mix than the unbounded 96 registers)
+__global__ void __launch_bounds__(T2D_MAX, 6) k_cells2d_mixed(const Cell2DArgs A) {
     extern __shared__ double smem[];
     constexpr int CAP = CAP_FAST_2D;
     const int t = threadIdx.x, T2D = blockDim.x;
