@@ -128,23 +128,40 @@ __global__ void k_tree_init(TreeNode<D> *nodes, int *level, int *counters, int n
     for (int p = 3; p < npass + 3; ++p) counters[p] = 1;
 }
 
-__device__ __forceinline__ int lower_bound_key(const unsigned *keys, int a, int b, unsigned long long v) {
-    while (a < b) {
-        int m = (a + b) >> 1;
-        if ((unsigned long long)keys[m] < v)
-            a = m + 1;
-        else
-            b = m;
+// First index of [lo, hi) whose key is >= v, found by the 32 lanes of a warp
+// together (every lane gets it): each round probes 32 evenly spaced keys and
+// keeps the stretch between the last one below v and the next, so a range of
+// r keys takes about log32(r) dependent reads instead of log2(r).
+__device__ __forceinline__ int warp_lower_bound(const unsigned *keys, int lo, int hi, unsigned long long v) {
+    const int lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const int step = (hi - lo + 31) / 32;
+        const int i = lo + lane * step;
+        const bool below = i < hi && (unsigned long long)keys[i] < v;
+        const int cnt = __popc(__ballot_sync(0xffffffffu, below));  // probes 0 .. cnt - 1 are below v
+        if (cnt == 0) return lo;
+        const int nlo = lo + (cnt - 1) * step + 1;
+        const int nhi = lo + cnt * step;
+        lo = nlo;
+        if (nhi < hi) hi = nhi;
     }
-    return a;
+    const int i = lo + lane;
+    const bool below = i < hi && (unsigned long long)keys[i] < v;
+    return lo + __popc(__ballot_sync(0xffffffffu, below));
 }
 
+// One level of the top-down split, one warp per node of the level: the node's
+// key range is cut at the 2^D child prefixes of its next Morton level (single-
+// child levels skipped); children are appended at the node counter.
 template <int D>
 __global__ void k_split(TreeNode<D> *nodes, int *level, int *counters, int pass, const unsigned *keys, int bits,
                         int max_per_leaf, int max_nodes) {
     const int beg = counters[1 + pass], end = counters[2 + pass];
     constexpr int C = 1 << D;
-    for (int node = beg + blockIdx.x * blockDim.x + threadIdx.x; node < end; node += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int warp = int((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = int((gridDim.x * (long long)blockDim.x) >> 5);
+    for (int node = beg + warp; node < end; node += nwarps) {
         int a = nodes[node].a, b = nodes[node].b, L = level[node];
         while (true) {
             if (b - a <= max_per_leaf || L >= bits) break;  // leaf
@@ -154,29 +171,33 @@ __global__ void k_split(TreeNode<D> *nodes, int *level, int *counters, int pass,
             st[0] = a;
             st[C] = b;
             for (int c = 1; c < C; ++c)
-                st[c] = lower_bound_key(keys, st[c - 1], b, ((prefix << D) | (unsigned long long)c) << shift);
+                st[c] = warp_lower_bound(keys, st[c - 1], b, ((prefix << D) | (unsigned long long)c) << shift);
             int ne = 0;
             for (int c = 0; c < C; ++c) ne += st[c + 1] > st[c];
             if (ne == 1) {
                 ++L;
                 continue;
             }
-            int first = atomicAdd(&counters[0], ne);
+            int first = 0;
+            if (lane == 0) first = atomicAdd(&counters[0], ne);
+            first = __shfl_sync(0xffffffffu, first, 0);
             if (first + ne > max_nodes) break;  // cannot happen: nodes <= 2n
-            int k = 0;
-            for (int c = 0; c < C; ++c) {
-                if (st[c + 1] > st[c]) {
-                    nodes[first + k].a = st[c];
-                    nodes[first + k].b = st[c + 1];
-                    level[first + k] = L + 1;
-                    ++k;
+            if (lane == 0) {
+                int k = 0;
+                for (int c = 0; c < C; ++c) {
+                    if (st[c + 1] > st[c]) {
+                        nodes[first + k].a = st[c];
+                        nodes[first + k].b = st[c + 1];
+                        level[first + k] = L + 1;
+                        ++k;
+                    }
                 }
+                nodes[node].a = first;
+                nodes[node].b = -ne;
             }
-            nodes[node].a = first;
-            nodes[node].b = -ne;
             break;
         }
-        level[node] = L;
+        if (lane == 0) level[node] = L;
     }
 }
 
