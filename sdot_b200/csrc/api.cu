@@ -25,7 +25,16 @@ using namespace sdot;
 
 namespace sdot {
 static std::atomic<unsigned long long> g_launches{0};
-void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local unsigned long long *t_capture = nullptr;
+void note_launch() {
+    if (t_capture)
+        ++*t_capture;
+    else
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+void note_launches(unsigned long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+CaptureCount::CaptureCount() : prev(t_capture) { t_capture = &n; }
+CaptureCount::~CaptureCount() { t_capture = prev; }
 }  // namespace sdot
 
 namespace {

@@ -116,6 +116,18 @@ struct PerDevice {
 
 // Process-wide count of this library's kernel launches (sdot_kernel_launches).
 void note_launch();
+void note_launches(unsigned long long k);
+// While one of these lives, the launches this thread notes are counted into
+// it instead (a stream capture: they run, and are counted, when the graph
+// is launched).
+struct CaptureCount {
+    unsigned long long n = 0;
+    unsigned long long *prev;
+    CaptureCount();
+    ~CaptureCount();
+    CaptureCount(const CaptureCount &) = delete;
+    CaptureCount &operator=(const CaptureCount &) = delete;
+};
 
 // Per-cell kernel bodies are device functions; a host build of them (for
 // CPU-side debugging of the kernels) is compiled with SDOT_HOST_KERNELS.

@@ -258,6 +258,46 @@ int grid_for(long long n, int tb) {
     return int(g);
 }
 
+// Captures the launches `f` makes on `st` into an executable graph; false
+// (nothing launched, nothing captured) where the stream cannot be captured:
+// the legacy default stream, or a stream already being captured.
+template <class F>
+bool capture(cudaStream_t st, cudaGraphExec_t &exec, unsigned long long &launches, F &&f) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaGraph_t g = nullptr;
+    unsigned long long counted = 0;
+    {
+        CaptureCount cc;
+        try {
+            f();
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        counted = cc.n;
+    }
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (e == cudaSuccess && g) e = cudaGraphInstantiate(&exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        exec = nullptr;
+        return false;
+    }
+    launches = counted;
+    return true;
+}
+
 }  // namespace
 
 template <int D>
@@ -288,7 +328,16 @@ void DeviceTree<D>::reserve(long long nn) {
 }
 
 template <int D>
+void DeviceTree<D>::drop_graphs() {
+    if (build_graph) cudaGraphExecDestroy(build_graph);
+    if (weights_graph) cudaGraphExecDestroy(weights_graph);
+    build_graph = weights_graph = nullptr;
+    bg_n = wg_n = -1;
+}
+
+template <int D>
 void DeviceTree<D>::release() {
+    drop_graphs();
     dev_free(pos); dev_free(w); dev_free(idx); dev_free(inv);
     dev_free(nodes); dev_free(node_level); dev_free(counters);
     dev_free(keys); dev_free(keys2); dev_free(keys3);
@@ -304,6 +353,25 @@ void DeviceTree<D>::build(const double *pos_orig, const double *w_orig, long lon
     reserve(nn);
     n = nn;
     if (n == 0) return;
+    if (!(build_graph && bg_n == n && bg_pos == pos_orig && bg_w == w_orig && bg_leaf == max_per_leaf)) {
+        if (build_graph) cudaGraphExecDestroy(build_graph);
+        build_graph = nullptr;
+        bg_n = -1;
+        if (!capture(st, build_graph, bg_launches, [&] { build_launches(pos_orig, w_orig, st); })) {
+            build_launches(pos_orig, w_orig, st);
+            return;
+        }
+        bg_n = n;
+        bg_pos = pos_orig;
+        bg_w = w_orig;
+        bg_leaf = max_per_leaf;
+    }
+    SDOT_CUDA(cudaGraphLaunch(build_graph, st));
+    note_launches(bg_launches);
+}
+
+template <int D>
+void DeviceTree<D>::build_launches(const double *pos_orig, const double *w_orig, cudaStream_t st) {
     k_bbox_init<D><<<1, 32, 0, st>>>(bbox_bits);
     note_launch();
     k_bbox<D><<<grid_for(n, TB), TB, 0, st>>>(pos_orig, n, bbox_bits);
@@ -335,6 +403,23 @@ void DeviceTree<D>::build(const double *pos_orig, const double *w_orig, long lon
 template <int D>
 void DeviceTree<D>::update_weights(const double *w_orig, cudaStream_t st) {
     if (n == 0) return;
+    if (!(weights_graph && wg_n == n && wg_w == w_orig)) {
+        if (weights_graph) cudaGraphExecDestroy(weights_graph);
+        weights_graph = nullptr;
+        wg_n = -1;
+        if (!capture(st, weights_graph, wg_launches, [&] { weights_launches(w_orig, st); })) {
+            weights_launches(w_orig, st);
+            return;
+        }
+        wg_n = n;
+        wg_w = w_orig;
+    }
+    SDOT_CUDA(cudaGraphLaunch(weights_graph, st));
+    note_launches(wg_launches);
+}
+
+template <int D>
+void DeviceTree<D>::weights_launches(const double *w_orig, cudaStream_t st) {
     k_gather_w<D><<<ceil_div(n, TB), TB, 0, st>>>(w_orig, idx, n, w);
     note_launch();
     refresh_maxw(st);

@@ -49,8 +49,21 @@ struct DeviceTree {
     double *bbox = nullptr;   // 2 * D doubles (min, max) of the positions
     unsigned long long *bbox_bits = nullptr;
 
+    // build() and update_weights() replay their launches from CUDA graphs,
+    // captured on the first call for the same input buffers, size and leaf
+    // size (about 80 and 20 small launches; direct launches where the stream
+    // cannot be captured)
+    cudaGraphExec_t build_graph = nullptr, weights_graph = nullptr;
+    const void *bg_pos = nullptr, *bg_w = nullptr, *wg_w = nullptr;
+    long long bg_n = -1, wg_n = -1;
+    int bg_leaf = -1;
+    unsigned long long bg_launches = 0, wg_launches = 0;
+
     void reserve(long long n);
     void release();
+    void drop_graphs();
+    void build_launches(const double *pos_orig, const double *w_orig, cudaStream_t st);
+    void weights_launches(const double *w_orig, cudaStream_t st);
     // positions (D * n, AoS) and weights in original order, device pointers
     void build(const double *pos_orig, const double *w_orig, long long n, cudaStream_t st);
     // new weights (original order, device pointer): re-gather and refresh maxw
