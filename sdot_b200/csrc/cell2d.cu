@@ -496,9 +496,12 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
             nd_a = nd.a;
             nd_b = nd.b;
         }
-        // ---- the vertex pass shared by both kinds of step (bit k: vertex k
-        // is outside the bisector, or fails the eviction test)
+        // ---- the pass over the vertices: a cut classifies each vertex by
+        // its side of the bisector (bit k: vertex k outside); a node test
+        // stops at the first vertex that fails the eviction test, as the
+        // reference's all_pos does (mask 1: the box is needed)
         unsigned mask = 0;
+        int tested = n;
         if (is_cut) {
             for (int k = 0; k < n; ++k) {
                 const double d = (ox - cell.X(k)) * nx + (oy - cell.Y(k)) * ny;
@@ -512,13 +515,15 @@ SDOT_KFN int build_cell(const Cell2DArgs &A, long long s, const PolyView<double>
                 const double rhs = (qx - px) * (qx - px) + (qy - py) * (qy - py) - maxw;
                 if (!(lhs <= rhs)) {  // this vertex fails: the box is needed
                     mask = 1u;
+                    tested = k + 1;
                     break;
                 }
             }
         }
+        (void)tested;
         const CutFacts f = cut_facts(mask, n);
         SDOT_WORK_ADD(is_cut ? 0 : 2, 1);
-        SDOT_WORK_ADD(is_cut ? 1 : 3, n);
+        SDOT_WORK_ADD(is_cut ? 1 : 3, tested);
         if (is_cut) {
             if (f.nb_out) {
                 SDOT_WORK_ADD(4, 1);

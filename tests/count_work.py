@@ -7,7 +7,8 @@
 Runs one evaluation of the 1M-Dirac 2D clustered mix with the counting build
 (-DSDOT_COUNT), which adds up the work of the fast tier's walks: cut attempts,
 vertices classified at each attempt, node (eviction) tests and the vertices
-tested at each, effective cuts, final vertices.  With the operation weights of
+tested at each (up to the first that fails, as the reference's all_pos
+stops), effective cuts, final vertices.  With the operation weights of
 the reference algorithm (FMA = 2 flops: bisector setup 12 per attempt, signed
 distance 5 per vertex per attempt, eviction test 12 per vertex tested, area +
 centroid 20 and boundary + Hessian term 15 per final vertex) it writes the
