@@ -710,7 +710,7 @@ struct sdot_ctx {
             cells2d_launch(a, scratch, stream);
         }
         SDOT_CUDA(cudaEventRecord(ev[2], stream));
-        csr_sort_merge(rows, n, perm(), cnt_orig, stream);
+        csr_sort_merge(rows, n, perm(), cnt_orig, dim == 2, stream);
         scan_exclusive_total<long long>(cnt_orig, offsets, n, scan_tmp, stream);
         unpermute(s_mass, o_mass, n, 1, perm(), stream);
         unpermute(s_mass_c, o_mass_c, n, 1, perm(), stream);

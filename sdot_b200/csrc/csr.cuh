@@ -10,7 +10,8 @@ namespace sdot {
 // values of equal columns are summed in ascending value order.  Rewrites the
 // rows in place and stores the merged count both in R.cnt[s] (rows keep
 // their storage) and in cnt_orig[idx[s]] (original order, for the scan).
-void csr_sort_merge(const Rows &R, long long n, const int *idx, long long *cnt_orig, cudaStream_t st);
+// short_rows: stage rows of at most 16 entries in shared memory (2D rows)
+void csr_sort_merge(const Rows &R, long long n, const int *idx, long long *cnt_orig, bool short_rows, cudaStream_t st);
 // Write rows to CSR in original order: columns as original indices (int64).
 void csr_write(const Rows &R, long long n, const int *idx, const long long *offsets, long long *cols, double *vals,
                cudaStream_t st);
