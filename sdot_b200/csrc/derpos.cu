@@ -12,7 +12,7 @@
 // + p1 p0') (ConvexPolyhedron2.tcc:437-478); the row items are the reference's
 // 3 x 3 blocks (rows: centroid x, centroid y, mass; columns: position x,
 // position y, weight), corrected by the centroid and divided by
-// mass + (mass == 1) as the reference divides (.h:176-181), sorted by column
+// mass + (mass == 1) as the reference divides (.h:178-182), sorted by column
 // and merged.  One thread per cell; cells of more than DP_CAP vertices report
 // a capacity error.
 #include "derpos.cuh"
@@ -160,7 +160,7 @@ __device__ long long edge_block(const DpArgs &A, const CellGeo &g, int i0, doubl
     return A.idx[j];
 }
 
-// centroid correction, as the reference divides (.h:176-181)
+// centroid correction, as the reference divides (.h:178-182)
 __device__ void correct(const CellGeo &g, double *t) {
     const double div = g.mass + (g.mass == 1);
     const double c[2] = {g.cx, g.cy};
