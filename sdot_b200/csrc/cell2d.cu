@@ -680,23 +680,35 @@ SDOT_KFN int build_cell_f32(const Cell2DArgs &A, long long s, const PolyView<flo
             nd_a = nd.a;
             nd_b = nd.b;
         }
+        // a cut classifies every vertex (and flags one too close to call);
+        // a node test stops at the first vertex that fails the eviction
+        // test by more than its rounding margin (mask 1: the box is needed)
         unsigned mask = 0;
         bool near = false;
-        for (int k = 0; k < n; ++k) {
-            const float px = cell.X(k), py = cell.Y(k);
-            const float ex = ox - px, ey = oy - py;
-            const float d = ex * nx + ey * ny;
-            const float qx = fminf(hi0, fmaxf(lo0, px)) - px, qy = fminf(hi1, fmaxf(lo1, py)) - py;
-            const float uu = px * px + py * py, qq = qx * qx + qy * qy;
-            const float lhs = uu - w0f, rhs = qq - maxw;
-            const float emargin = F32_MARGIN * (uu + fabsf(w0f) + qq + fabsf(maxw));
-            const bool o = is_cut ? d < 0.0f : !(lhs <= rhs - emargin);
-            // rounding of d: the products, the bisector's origin, and the
-            // vertex, whose error scales with the edges it was cut from
-            near |= is_cut && fabsf(d) <= F32_MARGIN * (fabsf(ex * nx) + fabsf(ey * ny) +
-                                                        (fabsf(ox) + fabsf(px) + span) * fabsf(nx) +
-                                                        (fabsf(oy) + fabsf(py) + span) * fabsf(ny));
-            mask |= unsigned(o) << k;
+        if (is_cut) {
+            for (int k = 0; k < n; ++k) {
+                const float px = cell.X(k), py = cell.Y(k);
+                const float ex = ox - px, ey = oy - py;
+                const float d = ex * nx + ey * ny;
+                // rounding of d: the products, the bisector's origin, and the
+                // vertex, whose error scales with the edges it was cut from
+                near |= fabsf(d) <= F32_MARGIN * (fabsf(ex * nx) + fabsf(ey * ny) +
+                                                  (fabsf(ox) + fabsf(px) + span) * fabsf(nx) +
+                                                  (fabsf(oy) + fabsf(py) + span) * fabsf(ny));
+                mask |= unsigned(d < 0.0f) << k;
+            }
+        } else {
+            for (int k = 0; k < n; ++k) {
+                const float px = cell.X(k), py = cell.Y(k);
+                const float qx = fminf(hi0, fmaxf(lo0, px)) - px, qy = fminf(hi1, fmaxf(lo1, py)) - py;
+                const float uu = px * px + py * py, qq = qx * qx + qy * qy;
+                const float lhs = uu - w0f, rhs = qq - maxw;
+                const float emargin = F32_MARGIN * (uu + fabsf(w0f) + qq + fabsf(maxw));
+                if (!(lhs <= rhs - emargin)) {
+                    mask = 1u;
+                    break;
+                }
+            }
         }
         if (near) return -3;
         const CutFacts f = cut_facts(mask, n);
