@@ -56,10 +56,9 @@ def flops_per_cell_2d():
         with open(os.path.join(ROOT, "profiles", "work_counts_c2_1M.json")) as f:
             return float(json.load(f)["flops_per_cell"]), "measured on the benchmark input (tests/count_work.py)"
     except (OSError, KeyError, ValueError):
-        return 3.9e3, "uniform-input count (the benchmark input's count is absent)"
+        return 3.9e3, "uniform-input count of the earlier kernel (the benchmark input's count is absent)"
 
 
-FLOPS_PER_CELL = 3.9e3
 # per-cell algorithmic HBM bytes: positions + weight in (24), area (8),
 # centroid (16), ~7 Hessian entries x 12 + offset 8
 BYTES_PER_CELL = 136.0
