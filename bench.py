@@ -71,7 +71,7 @@ BYTES_PER_CELL_3D = 264.0
 
 
 def hbm_peak():
-    """Measured HBM copy bandwidth of this GPU pool (GB/s), else the fallback figure."""
+    """Measured HBM copy bandwidth of these B200s (GB/s), else the fallback figure."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"])

@@ -5,7 +5,7 @@ get_integrals / get_centroids / get_der_integrals_wrt_weights over
 ConvexPolyhedronAssembly or ScaledImage bounds), compiled by oracle/Makefile
 from the reference sources with the driver oracle/ref_driver.cpp.  Only
 tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the
-checker and the timed CPU baseline.
+parity reference and the timed CPU baseline.
 """
 import ctypes
 import os

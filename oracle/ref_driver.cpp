@@ -1,6 +1,6 @@
 // C-ABI driver around the UNMODIFIED reference sdot headers.
 //
-// Test infrastructure only (the checker and the timed CPU baseline): it is
+// Test infrastructure only (the parity reference and the timed CPU baseline): it is
 // compiled by oracle/Makefile, with the reference sources included from where
 // they lie, into oracle/_ref/libsdot_ref.so.  Nothing in the product links it.
 //

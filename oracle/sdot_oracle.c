@@ -1,7 +1,7 @@
 /*
  * sdot_oracle.c -- CPU restatement of the reference's 2D power-diagram path.
  *
- * TEST INFRASTRUCTURE ONLY (the checker; see sdot_oracle.h).  Pinned by
+ * TEST INFRASTRUCTURE ONLY (the parity reference; see sdot_oracle.h).  Pinned by
  * tests/test_oracle_kat.py against the known answers of the reference's own
  * tests (tests/test_ConvexPolyhedron2.cpp, tests/test_scaled_image.cpp) and,
  * where the reference compiles, against its outputs on seeded inputs.

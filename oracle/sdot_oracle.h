@@ -1,7 +1,7 @@
 /*
  * sdot_oracle.h -- CPU restatement of the reference's power-diagram path.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker: tests/, the smoke test of
+ * TEST INFRASTRUCTURE ONLY.  This is the parity reference: tests/, the smoke test of
  * __graft_entry__ and bench.py's CPU-baseline leg may call it; the product
  * (sdot_b200/, libsdot_b200.so) never links or calls it.
  *
