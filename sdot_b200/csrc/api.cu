@@ -340,6 +340,8 @@ struct sdot_ctx {
         guard = nullptr;
         dfree(stage_i); dfree(stage_v);
         stage_cap = 0;
+        dfree(dp_off); dfree(dp_col); dfree(dp_val); dfree(dp_v);
+        dp_ncap = dp_nnzcap = 0;
         if (scratch3) cudaFree(scratch3);
         scratch3 = nullptr;
         if (scratch) cudaFree(scratch);
@@ -893,6 +895,26 @@ struct sdot_ctx {
     void mark_dirty() { eval_dirty = nb_dirty = true; }
 
     // staging buffers of at least `count` entries (25% headroom when grown)
+    // host-side outputs of the position derivatives: device staging kept
+    // and grown like the Hessian's (3 n + 1 offsets, nnz entries, 3 n values)
+    long long *dp_off = nullptr, *dp_col = nullptr;
+    double *dp_val = nullptr, *dp_v = nullptr;
+    long long dp_ncap = 0, dp_nnzcap = 0;
+    void reserve_derpos(long long nn, long long nnz) {
+        if (nn > dp_ncap || !dp_off) {
+            const long long c = nn + nn / 4 + 16;
+            dalloc(dp_off, size_t(3 * c + 1));
+            dalloc(dp_v, size_t(3 * c));
+            dp_ncap = c;
+        }
+        if (nnz > dp_nnzcap || !dp_col) {
+            const long long c = nnz + nnz / 4 + 1024;
+            dalloc(dp_col, size_t(c));
+            dalloc(dp_val, size_t(c));
+            dp_nnzcap = c;
+        }
+    }
+
     void reserve_stage(long long count) {
         if (count <= stage_cap && stage_i) return;
         const long long cap2 = count + count / 4 + 1024;
@@ -1691,32 +1713,21 @@ int sdot_get_der_centroids_and_integrals_wrt_weight_and_positions(sdot_ctx *ctx,
         if (!offsets || !values || !v_values) throw BadArg("null output");
         long long *d_off = reinterpret_cast<long long *>(offsets), *d_col = reinterpret_cast<long long *>(columns);
         double *d_val = values, *d_v = v_values;
-        // one-off host staging, freed on every exit
-        struct Staging {
-            long long *off = nullptr, *col = nullptr;
-            double *val = nullptr, *v = nullptr;
-            ~Staging() { dfree(off); dfree(col); dfree(val); dfree(v); }
-        } stg;
-        long long *&t_off = stg.off, *&t_col = stg.col;
-        double *&t_val = stg.val, *&t_v = stg.v;
         if (mem_space != SDOT_DEVICE) {
-            dalloc(t_off, size_t(3 * n + 1));
-            dalloc(t_col, size_t(std::max<long long>(nnz, 1)));
-            dalloc(t_val, size_t(std::max<long long>(nnz, 1)));
-            dalloc(t_v, size_t(3 * n));
-            d_off = t_off;
-            d_col = t_col;
-            d_val = t_val;
-            d_v = t_v;
+            ctx->reserve_derpos(n, nnz);
+            d_off = ctx->dp_off;
+            d_col = ctx->dp_col;
+            d_val = ctx->dp_val;
+            d_v = ctx->dp_v;
         }
         derpos_write(ctx->nb, n, ctx->tree2.pos, ctx->tree2.w, ctx->perm(), ctx->start_n, ctx->d_start, ctx->coeff,
                      int(ctx->trans_h.size() / 2), ctx->d_trans, boff, d_off, d_col, d_val, d_v, ctx->stream);
         if (mem_space != SDOT_DEVICE) {
-            SDOT_CUDA(cudaMemcpyAsync(offsets, t_off, size_t(3 * n + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
+            SDOT_CUDA(cudaMemcpyAsync(offsets, d_off, size_t(3 * n + 1) * sizeof(long long), cudaMemcpyDeviceToHost,
                                       ctx->stream));
-            SDOT_CUDA(cudaMemcpyAsync(columns, t_col, size_t(nnz) * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
-            SDOT_CUDA(cudaMemcpyAsync(values, t_val, size_t(nnz) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            SDOT_CUDA(cudaMemcpyAsync(v_values, t_v, size_t(3 * n) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(columns, d_col, size_t(nnz) * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(values, d_val, size_t(nnz) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            SDOT_CUDA(cudaMemcpyAsync(v_values, d_v, size_t(3 * n) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         }
         SDOT_CUDA(cudaStreamSynchronize(ctx->stream));
         *nnz_inout = nnz;
