@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--config", default="c2", choices=["c2", "c4"],
                     help="c2: 2D 1M clustered mix (the headline); c4: 3D 200k uniform + jittered lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true",
+                    help="skip the mixed-precision and Newton legs run after the timed region (a bounded "
+                         "launch list of the bench command)")
     ap.add_argument("--serving", action="store_true",
                     help="serving benchmark: a Poisson stream of OT solves, continuous batching vs sequential")
     ap.add_argument("--requests", type=int, default=200)
@@ -433,7 +436,7 @@ def run_ours(args):
            "stages_ms": {"cells": cell}}
     # ---- outside the timed region: the mixed-precision path on the same
     # problem (cells/s and its error against the FP64 path) and Newton times
-    if rank == 0 and world == 1 and dim == 2:
+    if rank == 0 and world == 1 and dim == 2 and not args.no_extra_legs:
         try:
             out["mixed"] = mixed_leg(L, c, n, dev, flush, args.steps)
         except Exception as e:  # reported, never required
